@@ -1,0 +1,169 @@
+/*
+ * tdfcuda.h -- C ABI of libtdfcuda, the B200 (sm_100a) engine for the
+ * coherent F-statistic search hot path of TDFstat: the per-sky-point
+ * job_core() chain of search/network/openmp.
+ *
+ * Plain C types only (pointers, sizes, scalars).  All input pointers are HOST
+ * pointers unless a name says otherwise; the library copies what it needs to
+ * the device.  Every function returns a tdf_status; tdf_last_error() gives a
+ * message for the calling thread's last failure.
+ *
+ * Reference interfaces replaced (paths relative to the TDFstat tree):
+ *   job_core()            search/network/openmp/jobcore.c:193-630,
+ *                         declared jobcore.h:21-33   -> tdf_search_points(),
+ *                         tdf_job_core_ref() / job_core() in tdfcuda_refabi.h
+ *   spindown_modulation() search/network/openmp/spinmod.c:17-538 (inside)
+ *   modvir()/rogcvir()    search/network/openmp/settings.c:226-294 (inside)
+ *   splintpad()/spline()  search/network/openmp/auxi.c:93-169 (inside)
+ *   FStat()               search/network/openmp/auxi.c:336-363 (inside)
+ * The driver loop search() (jobcore.c:28-188) stays on the host; it may call
+ * tdf_search_points() for a whole sky patch instead of job_core() per point.
+ */
+#ifndef TDFCUDA_H
+#define TDFCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDF_MAX_DETECTORS 8   /* MAX_DETECTORS, struct.h:8 */
+#define TDF_MAX_LINES 512     /* MAXL, struct.h:14 */
+#define TDF_NAVFSTAT 4096     /* NAVFSTAT, auxi.h:12 */
+
+typedef enum tdf_status {
+     TDF_OK = 0,
+     TDF_ERR_INVALID = 1,          /* bad argument, size or layout */
+     TDF_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+     TDF_ERR_TRIGGER_OVERFLOW = 3, /* > bufsize/2 triggers in one spindown (jobcore.c:586-590) */
+     TDF_ERR_OUT_OF_MEMORY = 4,
+     TDF_ERR_CAPACITY = 5,         /* caller's output arrays are too small */
+     TDF_ERR_UNSUPPORTED = 6,      /* size or option outside what this build handles */
+     TDF_ERR_NO_DEVICE = 7,
+     TDF_ERR_NOT_BUILT = 8         /* this entry point is not available in this build */
+} tdf_status;
+
+/* Arithmetic form of the engine. */
+typedef enum tdf_form {
+     /* FP64 sky stage (shift, phase, FFT interpolation, spline); FP32
+        resampled series, demodulation sincos, FFTs and F-statistic, with the
+        spindown phase argument formed and reduced mod 2*pi in FP64. */
+     TDF_FORM_SPLIT = 0,
+     /* every step in FP64: the reference's PREC=DOUBLE build */
+     TDF_FORM_FP64 = 1
+} tdf_form;
+
+/* One detector's inputs: the fields of ifo[n] (struct.h:36-55,157-172) that
+   job_core() reads. */
+typedef struct tdf_detector {
+     const float *xdat;     /* [N] time series, ifo[n].sig.xDat */
+     const double *detssb;  /* [3N] detector position w.r.t. the SSB, ifo[n].sig.DetSSB */
+     double sig2;           /* ifo[n].sig.sig2 = crf0 * var(xDat) (common.c:68-78) */
+     double sphir, cphir;   /* ifo[n].sig.sphir, cphir (common.c:123-124) */
+     double amod[9];        /* ifo[n].amod.c1..c9 from rogcvir (settings.c:226-248) */
+} tdf_detector;
+
+/* One data segment: Search_settings (struct.h:105-145) fields the path reads,
+   the aux arrays (struct.h:96-101) and the detectors. */
+typedef struct tdf_segment {
+     int32_t N;             /* samples */
+     int32_t nfft;          /* 2^ceil(log2 N) */
+     int32_t nfftf;         /* fftpad * nfft: spindown FFT length */
+     int32_t Ninterp;       /* interpftpad * nfft: interpolation FFT length */
+     int32_t interpftpad;   /* 2 (settings.c:56) */
+     int32_t nifo;          /* detectors, 1..TDF_MAX_DETECTORS */
+     double dt, oms, sepsm, cepsm, Smin, Smax;
+     double M[16];          /* grid generator matrix, column-major (jobcore.c:218-240) */
+     const double *cosmodf; /* [N] cos(omr*i) (init.c:232-237) */
+     const double *sinmodf; /* [N] sin(omr*i) */
+     tdf_detector det[TDF_MAX_DETECTORS];
+} tdf_segment;
+
+/* Search options: Command_line_opts / Search_range / Search_settings fields
+   the path reads. */
+typedef struct tdf_search_opts {
+     double thr;            /* opts->thr: trigger threshold on F */
+     int32_t fr[2];         /* s_range->fr: F-statistic bins [fr0, fr1] */
+     int32_t allsky;        /* opts->gtype == "allsky": spindown range per sky point
+                               from Smin/Smax (jobcore.c:399-411) */
+     int32_t blocks_avg;    /* opts->fstat_norm == "blocks_avg" (jobcore.c:513-515) */
+     float spndr[2];        /* s_range->spndr (non-allsky spindown range) */
+     float sstep;           /* s_range->sstep */
+     int32_t bufsize;       /* sett->bufsize: floats per record; at most bufsize/2 triggers */
+     int32_t numlines;      /* sett->numlines_band */
+     const double *lines;   /* [numlines][2] veto intervals in radians (sett->lines) */
+} tdf_search_opts;
+
+/* One output record: the Trigger compound (struct.h:211-215) with the hvl_t
+   replaced by an offset into the caller's pair array. */
+typedef struct tdf_record {
+     float m, n, s, ra, dec, fdot;
+     uint32_t len;          /* ffstat.len: floats, two per trigger (f, F) */
+     uint32_t pad;
+     int64_t offset;        /* index (in floats) of the first pair in pairs[] */
+} tdf_record;
+
+typedef struct tdf_engine tdf_engine;
+
+const char *tdf_status_string(int status);
+/* message of the calling thread's last failed call ("" if none) */
+const char *tdf_last_error(void);
+int tdf_device_count(int *count);
+
+/* Create an engine on CUDA device `device`: validates sizes, allocates the
+   device buffers for up to `max_sky_batch` sky points in flight (0 = library
+   default), uploads the segment's inputs.  Replaces the per-run setup that
+   job_core() relies on (init_arrays, plan_fftw: init.c:247-294,710-755). */
+int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts,
+                      int form, int device, int max_sky_batch, tdf_engine **out);
+
+/* Copy new inputs (same sizes as at creation) into the engine's device
+   buffers without allocating; e.g. the next segment of a run. */
+int tdf_engine_upload(tdf_engine *e, const tdf_segment *seg);
+
+int tdf_engine_destroy(tdf_engine *e);
+
+/* Run npts sky points (hemisphere pm[i], grid position mm[i], nn[i]); the
+   work of npts job_core() calls (jobcore.c:193-630).  Records come out in
+   the reference order (point, then spindown), one per spindown of every
+   point inside the sky ellipse; points outside it give none (jobcore.c:248).
+   sst may be NULL (start of the spindown range = spndr[0]) or hold the
+   restart spindown per point (s_range->sst, jobcore.c:208).
+   nrec_per_point (may be NULL) receives each point's record count (the
+   *FNum increment).  Returns TDF_ERR_CAPACITY with the needed sizes in
+   *nrec / *npairs if the caller's arrays are too small. */
+int tdf_search_points(tdf_engine *e, int npts, const int32_t *pm, const float *mm,
+                      const float *nn, const float *sst,
+                      tdf_record *recs, int64_t max_recs, int64_t *nrec,
+                      float *pairs, int64_t max_pairs, int64_t *npairs,
+                      int32_t *nrec_per_point);
+
+/* Device-only pass: same work as tdf_search_points() but the trigger list
+   stays on the device; returns the record and trigger counts.  Used to time
+   the kernels with inputs resident in HBM. */
+int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const float *mm,
+                             const float *nn, const float *sst,
+                             int64_t *nrec, int64_t *ntrig);
+
+/* The full F-statistic of one template (sky point, spindown ss) over bins
+   [fr0, fr1], after the optional blocks_avg normalisation: F[k - fr0]
+   (jobcore.c:481-515).  Returns TDF_ERR_INVALID if the point is outside the
+   sky ellipse. */
+int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss,
+                       double *F, int64_t nF);
+
+/* The CUDA stream the engine enqueues on (a cudaStream_t), and a way to make
+   it enqueue on the caller's stream instead (NULL = the engine's own). */
+int tdf_engine_get_stream(tdf_engine *e, void **stream);
+int tdf_engine_set_stream(tdf_engine *e, void *stream);
+
+/* Kernel launches issued by the engine since creation (for accounting). */
+int tdf_engine_launch_count(tdf_engine *e, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,127 @@
+"""ctypes mirror of include/tdfcuda.h (the C ABI of libtdfcuda).
+
+The structure layouts here must match the header field for field; the
+library checks ``sizeof`` of each at load time through
+``tdf_abi_struct_sizes``.
+"""
+import ctypes as C
+import os
+
+TDF_MAX_DETECTORS = 8
+TDF_MAX_LINES = 512
+TDF_NAVFSTAT = 4096
+
+TDF_OK = 0
+TDF_ERR_INVALID = 1
+TDF_ERR_CUDA = 2
+TDF_ERR_TRIGGER_OVERFLOW = 3
+TDF_ERR_OUT_OF_MEMORY = 4
+TDF_ERR_CAPACITY = 5
+TDF_ERR_UNSUPPORTED = 6
+TDF_ERR_NO_DEVICE = 7
+TDF_ERR_NOT_BUILT = 8
+
+TDF_FORM_SPLIT = 0
+TDF_FORM_FP64 = 1
+
+FORMS = {"split": TDF_FORM_SPLIT, "fp64": TDF_FORM_FP64}
+
+
+class TdfDetector(C.Structure):
+    _fields_ = [
+        ("xdat", C.POINTER(C.c_float)),
+        ("detssb", C.POINTER(C.c_double)),
+        ("sig2", C.c_double),
+        ("sphir", C.c_double),
+        ("cphir", C.c_double),
+        ("amod", C.c_double * 9),
+    ]
+
+
+class TdfSegment(C.Structure):
+    _fields_ = [
+        ("N", C.c_int32),
+        ("nfft", C.c_int32),
+        ("nfftf", C.c_int32),
+        ("Ninterp", C.c_int32),
+        ("interpftpad", C.c_int32),
+        ("nifo", C.c_int32),
+        ("dt", C.c_double),
+        ("oms", C.c_double),
+        ("sepsm", C.c_double),
+        ("cepsm", C.c_double),
+        ("Smin", C.c_double),
+        ("Smax", C.c_double),
+        ("M", C.c_double * 16),
+        ("cosmodf", C.POINTER(C.c_double)),
+        ("sinmodf", C.POINTER(C.c_double)),
+        ("det", TdfDetector * TDF_MAX_DETECTORS),
+    ]
+
+
+class TdfSearchOpts(C.Structure):
+    _fields_ = [
+        ("thr", C.c_double),
+        ("fr", C.c_int32 * 2),
+        ("allsky", C.c_int32),
+        ("blocks_avg", C.c_int32),
+        ("spndr", C.c_float * 2),
+        ("sstep", C.c_float),
+        ("bufsize", C.c_int32),
+        ("numlines", C.c_int32),
+        ("lines", C.POINTER(C.c_double)),
+    ]
+
+
+class TdfRecord(C.Structure):
+    _fields_ = [
+        ("m", C.c_float),
+        ("n", C.c_float),
+        ("s", C.c_float),
+        ("ra", C.c_float),
+        ("dec", C.c_float),
+        ("fdot", C.c_float),
+        ("len", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("offset", C.c_int64),
+    ]
+
+
+# (name, restype, argtypes) of every function include/tdfcuda.h declares
+P = C.c_void_p
+I32P = C.POINTER(C.c_int32)
+F32P = C.POINTER(C.c_float)
+F64P = C.POINTER(C.c_double)
+I64P = C.POINTER(C.c_int64)
+RECP = C.POINTER(TdfRecord)
+
+ABI_FUNCTIONS = [
+    ("tdf_status_string", C.c_char_p, [C.c_int]),
+    ("tdf_last_error", C.c_char_p, []),
+    ("tdf_device_count", C.c_int, [I32P]),
+    ("tdf_engine_create", C.c_int,
+     [C.POINTER(TdfSegment), C.POINTER(TdfSearchOpts), C.c_int, C.c_int, C.c_int, C.POINTER(P)]),
+    ("tdf_engine_upload", C.c_int, [P, C.POINTER(TdfSegment)]),
+    ("tdf_engine_destroy", C.c_int, [P]),
+    ("tdf_search_points", C.c_int,
+     [P, C.c_int, I32P, F32P, F32P, F32P, RECP, C.c_int64, I64P, F32P, C.c_int64, I64P, I32P]),
+    ("tdf_search_points_device", C.c_int,
+     [P, C.c_int, I32P, F32P, F32P, F32P, I64P, I64P]),
+    ("tdf_fstat_spectrum", C.c_int,
+     [P, C.c_int32, C.c_float, C.c_float, C.c_float, F64P, C.c_int64]),
+    ("tdf_engine_get_stream", C.c_int, [P, C.POINTER(P)]),
+    ("tdf_engine_set_stream", C.c_int, [P, P]),
+    ("tdf_engine_launch_count", C.c_int, [P, I64P]),
+]
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libtdfcuda.so")
+
+
+def bind(lib):
+    """Attach restype/argtypes of every ABI function to a loaded CDLL."""
+    for name, res, args in ABI_FUNCTIONS:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib

@@ -1,0 +1,392 @@
+"""Benchmark of the coherent-search hot path (job_core chain) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tdf|reference]
+                    [--form split|fp64] [--workload cfg2|cfg1|cfg3]
+
+Workload (default cfg2): H1+L1, 2-sidereal-day segment at dt = 2 s
+(N = 86164, nfft = nfftf = 2^17, Ninterp = 2^18), seeded Gaussian noise
+(sigma 1, 5% gaps) plus an injected CW signal (network SNR 12, f = 100.1234 Hz,
+fdot = -3e-10 Hz/s), a 32 x 32 sky patch around the injection x 401
+spindowns = 410,624 templates per step, F over bins [1024, 64512], thr 14.5.
+A step is one pass of the hot path over the whole patch.  Inputs are synthetic
+(no public data set is used).
+
+  value : templates/s with the segment resident in HBM (device-only pass:
+          sky stage + spindown stage + trigger compaction), CUDA events on
+          the engine's stream, barrier + synchronize around the K steps,
+          max over ranks.
+  e2e   : the same through the C ABI with host buffers: upload of the
+          segment's inputs (xdat, DetSSB, aux arrays) and download of the
+          records inside every step.
+  --impl reference: the reference's own C search (its unmodified sources,
+          PREC=FLOAT, built by oracle/Makefile) on the host cores, each step
+          a bounded sample (2 sky points x 401 spindowns) of the workload.
+Under torchrun (N > 1) the sky points are split into contiguous shards, one
+per rank (no collective on the data path); rank 0 prints the JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "templates/s (sky x spindown) on 1 B200, split-prec vs plain FP64 @<=1e-4 F err"
+UNIT = "templates/s"
+
+
+# ------------------------------------------------------------------ workload
+
+def workload_case(name: str):
+    from tdfstat_b200 import synth
+    if name == "cfg1":
+        return synth.Case(dt=2.0, nod=2, band=2880, dets=("H1",), read_o3=True, seed=101, thr=14.5,
+                          fdot_step=1e-10, sky_cells=16.0), (1, 1), 64, 0.25
+    if name == "cfg3":
+        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=1.9, dec=0.2, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+        return synth.Case(dt=2.0, nod=6, band=2880, dets=("H1", "L1"), seed=303, thr=14.5, fdot_step=1e-10,
+                          sky_cells=16.0, injections=(inj,)), (128, 64), 401, 0.25
+    inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=1.9, dec=0.2, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+    return synth.Case(dt=2.0, nod=2, band=2880, dets=("H1", "L1"), seed=202, thr=14.5, fdot_step=1e-10,
+                      sky_cells=16.0, injections=(inj,)), (32, 32), 401, 0.25
+
+
+class Workload:
+    def __init__(self, name: str, root: str):
+        from tdfstat_b200 import host, synth
+        case, (nm, nn_), nspd, step = workload_case(name)
+        self.name, self.case = name, case
+        inj = case.injections[0] if case.injections else None
+        c = case
+        # a directed_range INI centred on the injection (or a fixed point)
+        ra, dec = (inj.ra, inj.dec) if inj else (1.2, 0.3)
+        fdot = inj.fdot if inj else 0.0
+        st = c.settings()
+        c.gtype = "directed_range"
+        c.gcenter = (st.fpo + st.B / 2, fdot, ra, dec)
+        half = (nspd - 1) // 2
+        c.gsizes = (st.nfft // 4 - 1024, float(half), 0.0, 0.0)
+        c.gsteps = (1, 1.0, 1.0, 1.0)
+        ini = synth.write_case(root, c)
+        self.ini = ini
+        job = host.Job(ini, float_build=True)
+        self.job = job
+        # the F range of an all-sky run: [nmin, nmax]
+        job.range.fr = [job.sett.nmin, job.sett.nmax]
+        job.sett.bufsize = job.sett.nfftf
+        pm0, mm0, nn0 = job.sky_points()
+        m0, n0 = mm0[0], nn0[0]
+        self.pm = np.full(nm * nn_, pm0[0], dtype=np.int32)
+        mg, ng = np.meshgrid((np.arange(nm) - nm // 2) * step, (np.arange(nn_) - nn_ // 2) * step, indexing="ij")
+        self.mm = (m0 + mg.ravel()).astype(np.float32)
+        self.nn = (n0 + ng.ravel()).astype(np.float32)
+        self.nspd = nspd
+        self.templates = nm * nn_ * nspd
+        self.config = {"workload": name, "detectors": "".join(c.dets), "N": job.sett.N, "nfft": job.sett.nfft,
+                       "nfftf": job.sett.nfftf, "Ninterp": job.sett.Ninterp, "sky_points": nm * nn_,
+                       "spindowns": nspd, "templates_per_step": self.templates,
+                       "fr": list(job.range.fr), "thr": c.thr}
+
+    def shard(self, rank: int, world: int):
+        n = len(self.pm)
+        a, b = rank * n // world, (rank + 1) * n // world
+        return self.pm[a:b], self.mm[a:b], self.nn[a:b]
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=self.f, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for r in csv.reader(f):
+                if len(r) >= 9:
+                    rows.append([x.strip() for x in r])
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ helpers
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per template of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), if present."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_reference_sample(wl: Workload, root: str, npts: int, threads: int):
+    """Runs the reference FLOAT build on `npts` sky points of the workload
+    (directed_range patch of the same segment); returns (templates, seconds,
+    binary kind)."""
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import refkit
+    from tdfstat_b200 import synth
+    binp = refkit.REF_BIN["f32"]
+    if not os.path.exists(binp):
+        return None
+    c = wl.case
+    half = (wl.nspd - 1) // 2
+    c.gsizes = (wl.job.sett.nfft // 4 - 1024, float(half), 0.0, float((npts - 1) // 2))
+    c.gsteps = (1, 1.0, 1.0, 0.25)
+    ini = synth.write_case(root, c)
+    shutil.rmtree(os.path.join(root, "out"), ignore_errors=True)
+    os.makedirs(os.path.join(root, "out"), exist_ok=True)
+    recs, meta, _ = refkit.run_reference(ini, "f32", threads=threads)
+    return len(recs), float(meta["walltime"])
+
+
+# ------------------------------------------------------------------ arms
+
+def run_tdf(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from tdfstat_b200.engine import Engine, load_library
+    import ctypes as C
+
+    torch.cuda.set_device(local_rank)
+    root = tempfile.mkdtemp(prefix="tdfbench_")
+    try:
+        wl = Workload(args.workload, root)
+        job = wl.job
+        pm, mm, nn = wl.shard(rank, world)
+        seg, opts = job.segment(), job.search_opts()
+        eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
+        lib = load_library()
+        stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
+        ntmpl = len(pm) * wl.nspd
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+        def barrier():
+            if world > 1:
+                dist.barrier()
+
+        # warm-up (also compiles nothing: kernels are AOT sm_100a)
+        for _ in range(args.warmup):
+            eng.search_device(pm, mm, nn)
+        torch.cuda.synchronize()
+        # ---- value: device-resident inputs, K steps
+        eng.enable_kernel_timing(True)
+        launches0 = eng.launch_count()
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ntrig = 0
+        ev0.record(stream)
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()   # 256 MiB (> L2) written between steps, on the engine's stream
+            nrec, nt = eng.search_device(pm, mm, nn)
+            ntrig += nt
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+        ms = ev0.elapsed_time(ev1)
+        launches = eng.launch_count() - launches0
+        ktimes = eng.kernel_times()
+        eng.enable_kernel_timing(False)
+        # ---- e2e: host buffers through the C ABI
+        for _ in range(1):
+            eng.upload(seg)
+            eng.search(pm, mm, nn)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            eng.upload(seg)
+            res = eng.search(pm, mm, nn)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e = e0.elapsed_time(e1)
+        h2d = sum(d.xdat.nbytes + d.detssb.nbytes for d in job.dets) + job.cosmodf.nbytes + job.sinmodf.nbytes \
+            + pm.nbytes + mm.nbytes + nn.nbytes
+        d2h = len(res) * 40 + res.pairs_flat.nbytes
+        # max over ranks
+        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+        total_tmpl = len(wl.pm) * wl.nspd
+        value = total_tmpl * args.steps / (ms / 1e3)
+        e2e = total_tmpl * args.steps / (ms_e2e / 1e3)
+        out = None
+        if rank == 0:
+            peak, peak_kind = measured_peaks()
+            nifo = len(job.dets)
+            N = job.sett.N
+            bt = nifo * N * (24 if args.form == "split" else 40)   # algorithmic bytes per template
+            col_ms, col_n, col_t = ktimes["colpass_ms"], ktimes["colpass_launches"], ktimes["colpass_templates"]
+            roof = None
+            if col_n:
+                per_launch_bytes = bt * col_t / col_n
+                avg_s = col_ms / col_n / 1e3
+                achieved = per_launch_bytes / avg_s / 1e9
+                tr = profile_traffic()
+                traffic = None
+                if tr and tr.get("workload") == args.workload and tr.get("form") == args.form:
+                    traffic = tr["dram_bytes_per_template"] * col_t / col_n
+                roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4), "traffic": traffic,
+                        "kernel": "k_colpass (demodulation + first FFT pass)",
+                        "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                        "algorithmic_bytes_per_template": bt,
+                        "kernel_ms_share": {k: round(v, 3) for k, v in ktimes.items() if k.endswith("_ms")},
+                        "avg_launch_ms": round(col_ms / col_n, 4), "templates_per_launch": col_t / col_n}
+            cpu = None
+            if not args.no_cpu_baseline:
+                r = cpu_reference_sample(wl, tempfile.mkdtemp(prefix="tdfcpu_"), 3, os.cpu_count() or 1)
+                if r:
+                    nrec_c, secs = r
+                    cpu = {"value": round(nrec_c / secs, 2), "unit": UNIT, "cores": os.cpu_count(),
+                           "kind": "reference",
+                           "sample": "%d templates (3 sky points x %d spindowns) of the same workload, reference "
+                                     "search sources PREC=FLOAT built with the project FFTW-API shim "
+                                     "(textbook radix-2 FFT; FFTW absent), %.1f s" % (nrec_c, wl.nspd, secs)}
+            out = {
+                "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+                "scaling": "weak" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
+                "data": "synthetic (seeded Gaussian noise + injected CW signal, synthetic ephemeris)",
+                "config": dict(wl.config, form=args.form, l2="flush: 256 MiB write between timed steps; "
+                               "per-step working set > L2"),
+                "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches),
+                "triggers_per_step": int(ntrig // args.steps),
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            }
+        eng.close()
+        return out
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    root = tempfile.mkdtemp(prefix="tdfref_")
+    try:
+        wl = Workload(args.workload, root)
+        threads = os.cpu_count() or 1
+        sroot = tempfile.mkdtemp(prefix="tdfrefs_")
+        for _ in range(args.warmup):
+            r = cpu_reference_sample(wl, sroot, 1, threads)
+            if r is None:
+                return {"impl": "reference", "unavailable": "oracle/_ref/gwsearch-ref-f32 not built"}
+        tot_n, tot_s = 0, 0.0
+        for _ in range(args.steps):
+            n, s = cpu_reference_sample(wl, sroot, 1, threads)
+            tot_n += n
+            tot_s += s
+        v = tot_n / tot_s
+        sample = ("%d templates per step (1 sky point x %d spindowns) of the %s workload; reference search "
+                  "sources (PREC=FLOAT, SIMD=NONE) compiled unmodified against the project FFTW-API shim "
+                  "(textbook radix-2 FFT, FFTW absent)" % (tot_n // args.steps, wl.nspd, wl.name))
+        return {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * tot_s / args.steps, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": dict(wl.config),
+                "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tdf", choices=["tdf", "reference"])
+    ap.add_argument("--form", default="split", choices=["split", "fp64"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--sky-batch", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "tdf":
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_tdf(args, rank, world, local_rank)
+    if world > 1 and args.impl == "tdf":
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -162,6 +162,21 @@ int tdf_engine_set_stream(tdf_engine *e, void *stream);
 /* Kernel launches issued by the engine since creation (for accounting). */
 int tdf_engine_launch_count(tdf_engine *e, int64_t *count);
 
+/* Per-kernel device time, measured with CUDA events recorded on the
+   engine's stream around each launch while timing is on. */
+typedef struct tdf_kernel_times {
+     double colpass_ms;          /* demodulation + first FFT pass */
+     double rowpass_ms;          /* second FFT pass + F-statistic */
+     double threshold_ms;        /* local maxima, veto, trigger append */
+     double sky_ms;              /* whole sky stage */
+     int64_t colpass_launches, rowpass_launches, threshold_launches, sky_batches;
+     int64_t colpass_templates;  /* templates processed by the timed column passes */
+} tdf_kernel_times;
+
+/* on != 0 starts timing (and clears the accumulators); 0 stops it. */
+int tdf_engine_set_kernel_timing(tdf_engine *e, int on);
+int tdf_engine_get_kernel_times(tdf_engine *e, tdf_kernel_times *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,20 @@ class TdfRecord(C.Structure):
     ]
 
 
+class TdfKernelTimes(C.Structure):
+    _fields_ = [
+        ("colpass_ms", C.c_double),
+        ("rowpass_ms", C.c_double),
+        ("threshold_ms", C.c_double),
+        ("sky_ms", C.c_double),
+        ("colpass_launches", C.c_int64),
+        ("rowpass_launches", C.c_int64),
+        ("threshold_launches", C.c_int64),
+        ("sky_batches", C.c_int64),
+        ("colpass_templates", C.c_int64),
+    ]
+
+
 # (name, restype, argtypes) of every function include/tdfcuda.h declares
 P = C.c_void_p
 I32P = C.POINTER(C.c_int32)
@@ -112,6 +126,16 @@ ABI_FUNCTIONS = [
     ("tdf_engine_get_stream", C.c_int, [P, C.POINTER(P)]),
     ("tdf_engine_set_stream", C.c_int, [P, P]),
     ("tdf_engine_launch_count", C.c_int, [P, I64P]),
+    ("tdf_engine_set_kernel_timing", C.c_int, [P, C.c_int]),
+    ("tdf_engine_get_kernel_times", C.c_int, [P, C.POINTER(TdfKernelTimes)]),
+]
+
+# include/tdfcuda_refabi.h
+REFABI_FUNCTIONS = [
+    ("job_core", C.c_int, [C.c_int, C.c_float, C.c_float, P, P, P, P, P, P, I32P, P, I32P]),
+    ("tdf_job_core_ref", C.c_int, [C.c_int, C.c_float, C.c_float, P, P, P, P, P, P, I32P, P, I32P]),
+    ("tdf_job_core_release", None, []),
+    ("tdf_ref_struct_size", C.c_size_t, [C.c_int]),
 ]
 
 LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
@@ -120,7 +144,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libtdfcuda.so")
 
 def bind(lib):
     """Attach restype/argtypes of every ABI function to a loaded CDLL."""
-    for name, res, args in ABI_FUNCTIONS:
+    for name, res, args in ABI_FUNCTIONS + REFABI_FUNCTIONS:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

@@ -1,0 +1,961 @@
+// engine.cu -- libtdfcuda: the B200 engine behind include/tdfcuda.h.
+//
+// One engine = one data segment resident on one GPU.  A call runs a list of
+// sky points: the sky stage (FP64) for a batch of points, then every
+// template (point, spindown) of the batch through
+//   column pass  (demodulation fused into the first FFT pass)
+//   row pass     (second FFT pass + F-statistic)
+//   [block means](blocks_avg normalisation)
+//   threshold    (MAX_ALG 3 local maxima, veto, trigger append)
+// in chunks of templates.  Triggers are compacted on the device and sorted
+// into the reference's record order on the host.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "tdfcuda.h"
+#include "tdf_kernels.cuh"
+
+using namespace tdf;
+
+// ------------------------------------------------------------------ errors
+
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const char *fmt, ...) {
+     char buf[1024];
+     va_list ap;
+     va_start(ap, fmt);
+     vsnprintf(buf, sizeof(buf), fmt, ap);
+     va_end(ap);
+     g_last_error = buf;
+     return code;
+}
+
+#define CUCHK(x)                                                                          \
+     do {                                                                                 \
+          cudaError_t e_ = (x);                                                           \
+          if (e_ != cudaSuccess)                                                          \
+               return set_error(e_ == cudaErrorMemoryAllocation ? TDF_ERR_OUT_OF_MEMORY   \
+                                                                : TDF_ERR_CUDA,           \
+                                "%s: %s (%s:%d)", #x, cudaGetErrorString(e_), __FILE__,   \
+                                __LINE__);                                                \
+     } while (0)
+
+#define TRY(x)                        \
+     do {                             \
+          int s_ = (x);               \
+          if (s_ != TDF_OK) return s_; \
+     } while (0)
+
+// ------------------------------------------------------------------ launch helpers
+
+static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+static int ilog2i(int n) { int l = 0; while ((1 << l) < n) l++; return l; }
+
+template <class K>
+static int set_smem(K kern, size_t smem) {
+     if (smem > 48 * 1024) CUCHK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+     return TDF_OK;
+}
+
+template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
+static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
+     constexpr size_t smem = pass_smem_bytes<T, L, NA>();
+     auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi>;
+     TRY(set_smem(kern, smem));
+     kern<<<grid, L, smem, st>>>(pro, epi, tw);
+     CUCHK(cudaGetLastError());
+     return TDF_OK;
+}
+
+template <typename T, int L, int SIGN, int NA, class Src, class Epi>
+static int launch_row_L(dim3 grid, const Src &src, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
+     constexpr size_t smem = pass_smem_bytes<T, L, NA>();
+     auto kern = k_rowpass<T, L, SIGN, NA, Src, Epi>;
+     TRY(set_smem(kern, smem));
+     kern<<<grid, L, smem, st>>>(src, epi, tw);
+     CUCHK(cudaGetLastError());
+     return TDF_OK;
+}
+
+template <typename T, int SIGN, int NA, class Pro, class Epi>
+static int launch_col(int L, dim3 grid, const Pro &pro, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
+     switch (L) {
+     case 64: return launch_col_L<T, 64, SIGN, NA>(grid, pro, epi, tw, st);
+     case 128: return launch_col_L<T, 128, SIGN, NA>(grid, pro, epi, tw, st);
+     case 256: return launch_col_L<T, 256, SIGN, NA>(grid, pro, epi, tw, st);
+     case 512: return launch_col_L<T, 512, SIGN, NA>(grid, pro, epi, tw, st);
+     case 1024:
+          if constexpr (pass_smem_bytes<T, 1024, NA>() <= 227 * 1024)
+               return launch_col_L<T, 1024, SIGN, NA>(grid, pro, epi, tw, st);
+          else
+               return set_error(TDF_ERR_UNSUPPORTED, "column FFT of 1024 points not built for this form");
+     }
+     return set_error(TDF_ERR_UNSUPPORTED, "column FFT length %d", L);
+}
+
+template <typename T, int SIGN, int NA, class Src, class Epi>
+static int launch_row(int L, dim3 grid, const Src &src, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
+     switch (L) {
+     case 64: return launch_row_L<T, 64, SIGN, NA>(grid, src, epi, tw, st);
+     case 128: return launch_row_L<T, 128, SIGN, NA>(grid, src, epi, tw, st);
+     case 256: return launch_row_L<T, 256, SIGN, NA>(grid, src, epi, tw, st);
+     case 512: return launch_row_L<T, 512, SIGN, NA>(grid, src, epi, tw, st);
+     case 1024:
+          if constexpr (pass_smem_bytes<T, 1024, NA>() <= 227 * 1024)
+               return launch_row_L<T, 1024, SIGN, NA>(grid, src, epi, tw, st);
+          else
+               return set_error(TDF_ERR_UNSUPPORTED, "row FFT of 1024 points not built for this form");
+     }
+     return set_error(TDF_ERR_UNSUPPORTED, "row FFT length %d", L);
+}
+
+// ------------------------------------------------------------------ device buffers
+
+struct DevBuf {
+     void *p = nullptr;
+     size_t bytes = 0;
+     int alloc(size_t n) {
+          if (n <= bytes && p) return TDF_OK;
+          if (p) cudaFree(p);
+          p = nullptr;
+          bytes = 0;
+          if (n == 0) n = 16;
+          CUCHK(cudaMalloc(&p, n));
+          bytes = n;
+          return TDF_OK;
+     }
+     void release() {
+          if (p) cudaFree(p);
+          p = nullptr;
+          bytes = 0;
+     }
+     template <typename X> X *as() const { return reinterpret_cast<X *>(p); }
+};
+
+// twiddle tables of one four-step size N = N1*N2 in one precision
+template <typename T>
+struct FFTTables {
+     int N = 0, N1 = 0, N2 = 0;
+     DevBuf line1, line2, hi, lo;
+     int build(int n) {
+          N = n;
+          int l = ilog2i(n);
+          N1 = 1 << ((l + 1) / 2);
+          N2 = n / N1;
+          if (N1 < 64 || N2 < 64 || N1 > 1024 || N2 > 1024)
+               return set_error(TDF_ERR_UNSUPPORTED, "FFT length %d outside 2^12..2^20", n);
+          TRY(fill(line1, N1, N1));
+          TRY(fill(line2, N2, N2));
+          int nhi = std::max(1, n / 1024);
+          std::vector<cx<T>> h(nhi), o(1024);
+          for (int j = 0; j < nhi; j++) h[j] = tw((long)j * 1024, n);
+          for (int j = 0; j < 1024; j++) o[j] = tw(j, n);
+          TRY(hi.alloc(nhi * sizeof(cx<T>)));
+          TRY(lo.alloc(1024 * sizeof(cx<T>)));
+          CUCHK(cudaMemcpy(hi.p, h.data(), nhi * sizeof(cx<T>), cudaMemcpyHostToDevice));
+          CUCHK(cudaMemcpy(lo.p, o.data(), 1024 * sizeof(cx<T>), cudaMemcpyHostToDevice));
+          return TDF_OK;
+     }
+     static cx<T> tw(long m, long n) {
+          // e^{-2 pi i m/n}; m/n exact for power-of-two n
+          double a = -2.0 * M_PI * ((double)(m % n) / (double)n);
+          cx<T> r;
+          r.x = (T)std::cos(a);
+          r.y = (T)std::sin(a);
+          return r;
+     }
+     int fill(DevBuf &b, int L, int n) {
+          std::vector<cx<T>> v(L);
+          for (int m = 0; m < L; m++) v[m] = tw(m, n);
+          TRY(b.alloc(L * sizeof(cx<T>)));
+          CUCHK(cudaMemcpy(b.p, v.data(), L * sizeof(cx<T>), cudaMemcpyHostToDevice));
+          return TDF_OK;
+     }
+     void release() { line1.release(); line2.release(); hi.release(); lo.release(); }
+     const cx<T> *l1() const { return line1.as<cx<T>>(); }
+     const cx<T> *l2() const { return line2.as<cx<T>>(); }
+     const cx<T> *h() const { return hi.as<cx<T>>(); }
+     const cx<T> *o() const { return lo.as<cx<T>>(); }
+};
+
+// host view of one template
+struct HostTmpl {
+     int pt;         // index of the point in the call
+     float ss;
+     double spnd, het1;
+     double sgnl0;
+};
+
+struct HostPoint {
+     int inside = 0;
+     SkyParam sp;
+     float ra = 0, dec = 0;
+     float smin = 0;
+     int iss_size = 0;
+     int first_tmpl = 0;
+};
+
+struct tdf_engine {
+     int dev = 0, form = TDF_FORM_SPLIT;
+     cudaStream_t own = nullptr, stream = nullptr;
+     tdf_segment seg{};
+     tdf_search_opts opts{};
+     std::vector<double> lines;
+     std::vector<DetParam> dets;
+     int N = 0, nfft = 0, nfftf = 0, Ninterp = 0, nifo = 0, Nal = 0, n2N = 0;
+     int nF = 0, nblk_mu = 0;
+     int Bs = 8;        // sky points per batch
+     int Tc = 32;       // templates per chunk
+     int64_t launches = 0;
+     FFTTables<double> t_nfft, t_ninterp, t_f64;
+     FFTTables<float> t_f32;
+     // inputs
+     DevBuf xdat, detssb, cosm, sinm, pco, gco, detp;
+     // sky stage
+     DevBuf skyp, B0, B1, B2, shftf, partial, aabb;
+     // operands
+     DevBuf xab, s2, xa64, xb64, t1;
+     // spindown stage
+     DevBuf tparam, Ybuf, Fbuf, mubuf, trig, counters, tcnt, linesd;
+     unsigned long long trig_cap = 0;
+     // pinned staging
+     SkyParam *h_sky = nullptr;
+     TmplParam *h_tp = nullptr;
+     size_t h_tp_cap = 0;
+     unsigned long long *h_cnt = nullptr;
+     std::vector<Trig> h_trig;
+     // optional per-kernel event timing
+     bool timing = false;
+     tdf_kernel_times kt{};
+     std::vector<cudaEvent_t> evpool;
+     size_t evused = 0;
+     struct Pending { int kind; size_t ev; int64_t templates; };
+     std::vector<Pending> pending;
+};
+
+enum { KT_COL = 0, KT_ROW = 1, KT_THR = 2, KT_SKY = 3 };
+
+// records the opening event of a timed region; returns its pool index
+static size_t timing_begin(tdf_engine *e) {
+     if (e->evused + 2 > e->evpool.size()) {
+          for (int k = 0; k < 64; k++) {
+               cudaEvent_t ev;
+               if (cudaEventCreate(&ev) != cudaSuccess) break;
+               e->evpool.push_back(ev);
+          }
+     }
+     size_t i = e->evused;
+     if (i + 2 > e->evpool.size()) return (size_t)-1;
+     e->evused += 2;
+     cudaEventRecord(e->evpool[i], e->stream);
+     return i;
+}
+
+static void timing_end(tdf_engine *e, size_t i, int kind, int64_t templates) {
+     if (i == (size_t)-1) return;
+     cudaEventRecord(e->evpool[i + 1], e->stream);
+     e->pending.push_back({kind, i, templates});
+}
+
+// after a stream synchronisation: fold the recorded pairs into kt
+static void timing_collect(tdf_engine *e) {
+     for (const auto &p : e->pending) {
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, e->evpool[p.ev], e->evpool[p.ev + 1]) != cudaSuccess) continue;
+          switch (p.kind) {
+          case KT_COL: e->kt.colpass_ms += ms; e->kt.colpass_launches++; e->kt.colpass_templates += p.templates; break;
+          case KT_ROW: e->kt.rowpass_ms += ms; e->kt.rowpass_launches++; break;
+          case KT_THR: e->kt.threshold_ms += ms; e->kt.threshold_launches++; break;
+          case KT_SKY: e->kt.sky_ms += ms; e->kt.sky_batches++; break;
+          }
+     }
+     e->pending.clear();
+     e->evused = 0;
+}
+
+static size_t Wstride(const tdf_engine *e) { return (size_t)e->Ninterp; }
+
+// ------------------------------------------------------------------ setup
+
+static int validate(const tdf_segment *s, const tdf_search_opts *o) {
+     if (!s || !o) return set_error(TDF_ERR_INVALID, "null segment or options");
+     if (s->nifo < 1 || s->nifo > TDF_MAX_DETECTORS) return set_error(TDF_ERR_INVALID, "nifo=%d", s->nifo);
+     if (s->N < 2) return set_error(TDF_ERR_INVALID, "N=%d", s->N);
+     if (!pow2(s->nfft) || !pow2(s->nfftf) || !pow2(s->Ninterp))
+          return set_error(TDF_ERR_INVALID, "nfft/nfftf/Ninterp must be powers of two");
+     if (s->N > s->nfft || s->nfftf < s->nfft || s->Ninterp != s->interpftpad * s->nfft)
+          return set_error(TDF_ERR_INVALID, "inconsistent sizes N=%d nfft=%d nfftf=%d Ninterp=%d", s->N, s->nfft,
+                           s->nfftf, s->Ninterp);
+     if (s->interpftpad * s->N > s->Ninterp) return set_error(TDF_ERR_INVALID, "interpftpad*N > Ninterp");
+     if (s->nfft < 4096 || s->Ninterp > (1 << 20) || s->nfftf > (1 << 20))
+          return set_error(TDF_ERR_UNSUPPORTED, "FFT lengths must lie in 2^12..2^20");
+     if (o->fr[0] < 0 || o->fr[1] < o->fr[0] || o->fr[1] >= s->nfftf)
+          return set_error(TDF_ERR_INVALID, "fr range [%d, %d] outside [0, nfftf)", o->fr[0], o->fr[1]);
+     if (o->numlines < 0 || o->numlines > TDF_MAX_LINES || (o->numlines > 0 && !o->lines))
+          return set_error(TDF_ERR_INVALID, "numlines=%d", o->numlines);
+     if (!o->allsky && !(o->sstep > 0)) return set_error(TDF_ERR_INVALID, "sstep must be > 0");
+     if (o->bufsize < 2) return set_error(TDF_ERR_INVALID, "bufsize=%d", o->bufsize);
+     if (!s->cosmodf || !s->sinmodf) return set_error(TDF_ERR_INVALID, "null aux arrays");
+     for (int d = 0; d < s->nifo; d++)
+          if (!s->det[d].xdat || !s->det[d].detssb || !(s->det[d].sig2 > 0))
+               return set_error(TDF_ERR_INVALID, "detector %d: null input or sig2 <= 0", d);
+     return TDF_OK;
+}
+
+static int upload_inputs(tdf_engine *e, const tdf_segment *s) {
+     const int N = e->N, nifo = e->nifo;
+     for (int d = 0; d < nifo; d++) {
+          CUCHK(cudaMemcpyAsync(e->xdat.as<float>() + (size_t)d * e->Nal, s->det[d].xdat, N * sizeof(float),
+                                cudaMemcpyHostToDevice, e->stream));
+          CUCHK(cudaMemcpyAsync(e->detssb.as<double>() + (size_t)d * 3 * N, s->det[d].detssb, 3 * (size_t)N * sizeof(double),
+                                cudaMemcpyHostToDevice, e->stream));
+          DetParam &D = e->dets[d];
+          for (int k = 0; k < 9; k++) D.amod[k] = s->det[d].amod[k];
+          D.cphir = s->det[d].cphir;
+          D.sphir = s->det[d].sphir;
+          D.sig2 = s->det[d].sig2;
+     }
+     CUCHK(cudaMemcpyAsync(e->cosm.p, s->cosmodf, N * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+     CUCHK(cudaMemcpyAsync(e->sinm.p, s->sinmodf, N * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+     CUCHK(cudaMemcpyAsync(e->detp.p, e->dets.data(), nifo * sizeof(DetParam), cudaMemcpyHostToDevice, e->stream));
+     e->seg = *s;
+     return TDF_OK;
+}
+
+static int engine_alloc(tdf_engine *e) {
+     const int nifo = e->nifo, Bs = e->Bs, Tc = e->Tc;
+     const size_t Q = (size_t)Bs * nifo;
+     TRY(e->xdat.alloc((size_t)nifo * e->Nal * sizeof(float)));
+     CUCHK(cudaMemset(e->xdat.p, 0, e->xdat.bytes));
+     TRY(e->detssb.alloc((size_t)nifo * 3 * e->N * sizeof(double)));
+     TRY(e->cosm.alloc(e->N * sizeof(double)));
+     TRY(e->sinm.alloc(e->N * sizeof(double)));
+     TRY(e->detp.alloc(nifo * sizeof(DetParam)));
+     // spline recurrence factors (auxi.c:102-108): invp[i] = 2/(g[i-1]+4), g[i] = -0.5 invp[i]
+     {
+          const int n = e->n2N;
+          std::vector<double> p(n, 0.), g(n, 0.);
+          for (int i = 1; i < n - 1; i++) {
+               p[i] = 2. / (g[i - 1] + 4.);
+               g[i] = -.5 * p[i];
+          }
+          TRY(e->pco.alloc(n * sizeof(double)));
+          TRY(e->gco.alloc(n * sizeof(double)));
+          CUCHK(cudaMemcpy(e->pco.p, p.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+          CUCHK(cudaMemcpy(e->gco.p, g.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+     }
+     TRY(e->skyp.alloc(Bs * sizeof(SkyParam)));
+     const size_t ws = Wstride(e);
+     TRY(e->B0.alloc(Q * 2 * ws * sizeof(double2)));
+     TRY(e->B1.alloc(Q * 2 * ws * sizeof(double2)));
+     TRY(e->B2.alloc(Q * 2 * ws * sizeof(double2)));
+     TRY(e->shftf.alloc(Q * e->Nal * sizeof(double)));
+     TRY(e->partial.alloc(Q * (e->nfft / 256) * 2 * sizeof(double)));
+     TRY(e->aabb.alloc(Bs * sizeof(AaBb)));
+     const size_t ops = Q * e->Nal;
+     if (e->form == TDF_FORM_SPLIT) {
+          TRY(e->xab.alloc(ops * sizeof(float4)));
+          TRY(e->s2.alloc(ops * sizeof(float)));
+     } else {
+          TRY(e->xa64.alloc(ops * sizeof(double2)));
+          TRY(e->xb64.alloc(ops * sizeof(double2)));
+          TRY(e->t1.alloc(ops * sizeof(double)));
+     }
+     const size_t csz = e->form == TDF_FORM_SPLIT ? sizeof(float2) : sizeof(double2);
+     const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
+     TRY(e->Ybuf.alloc((size_t)Tc * 2 * e->nfftf * csz));
+     TRY(e->Fbuf.alloc((size_t)Tc * e->nF * rsz));
+     TRY(e->mubuf.alloc((size_t)Tc * std::max(1, e->nblk_mu) * rsz));
+     TRY(e->tcnt.alloc(Tc * sizeof(unsigned)));
+     TRY(e->counters.alloc(2 * sizeof(unsigned long long)));
+     TRY(e->linesd.alloc(std::max<size_t>(1, e->lines.size()) * sizeof(double)));
+     if (!e->lines.empty())
+          CUCHK(cudaMemcpy(e->linesd.p, e->lines.data(), e->lines.size() * sizeof(double), cudaMemcpyHostToDevice));
+     e->trig_cap = 1ull << 22;
+     TRY(e->trig.alloc(e->trig_cap * sizeof(Trig)));
+     CUCHK(cudaMallocHost((void **)&e->h_sky, Bs * sizeof(SkyParam)));
+     CUCHK(cudaMallocHost((void **)&e->h_cnt, 2 * sizeof(unsigned long long)));
+     TRY(e->t_nfft.build(e->nfft));
+     TRY(e->t_ninterp.build(e->Ninterp));
+     if (e->form == TDF_FORM_SPLIT) TRY(e->t_f32.build(e->nfftf));
+     else TRY(e->t_f64.build(e->nfftf));
+     return TDF_OK;
+}
+
+static void engine_free(tdf_engine *e) {
+     DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp,
+                       &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb, &e->xab, &e->s2,
+                       &e->xa64, &e->xb64, &e->t1, &e->tparam, &e->Ybuf, &e->Fbuf, &e->mubuf, &e->trig,
+                       &e->counters, &e->tcnt, &e->linesd};
+     for (DevBuf *b : bufs) b->release();
+     e->t_nfft.release();
+     e->t_ninterp.release();
+     e->t_f32.release();
+     e->t_f64.release();
+     if (e->h_sky) cudaFreeHost(e->h_sky);
+     if (e->h_tp) cudaFreeHost(e->h_tp);
+     if (e->h_cnt) cudaFreeHost(e->h_cnt);
+     e->h_sky = nullptr;
+     e->h_tp = nullptr;
+     e->h_cnt = nullptr;
+     for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
+     e->evpool.clear();
+     if (e->own) cudaStreamDestroy(e->own);
+     e->own = nullptr;
+}
+
+// ------------------------------------------------------------------ host-side per-point math
+
+// jobcore.c:243-262 (sky geometry) and 399-430 (spindown range), with the
+// reference's float/double types; `flt` selects FLOAT_TYPE = float.
+static void point_setup(const tdf_engine *e, int pm, float mm, float nn, float sst, HostPoint &P) {
+     const double *M = e->seg.M;
+     double al1 = nn * M[10] + mm * M[14];
+     double al2 = nn * M[11] + mm * M[15];
+     double cof = e->seg.oms;
+     P.inside = !(((al1 * al1) + (al2 * al2)) / (cof * cof) > 1.);
+     if (!P.inside) return;
+     double be1 = al1 / cof, be2 = al2 / cof;
+     double sindel = be1 * e->seg.sepsm - (2 * pm - 3) * std::sqrt(1. - be1 * be1 - be2 * be2) * e->seg.cepsm;
+     double cosdel = std::sqrt(1. - sindel * sindel);
+     double sinal = (be1 - e->seg.sepsm * sindel) / (e->seg.cepsm * cosdel);
+     double cosal = be2 / cosdel;
+     SkyParam &S = P.sp;
+     S.sinalt = sinal;
+     S.cosalt = cosal;
+     S.sindelt = sindel;
+     S.cosdelt = cosdel;
+     S.het0 = std::fmod(nn * M[8] + mm * M[12], M[0]);
+     S.nS0 = cosal * cosdel;
+     S.nS1 = sinal * cosdel;
+     S.nS2 = sindel;
+     // sgnlt[2..3] (FLOAT_TYPE) then the float record fields: one rounding
+     P.dec = (float)std::asin(sindel);
+     P.ra = (float)std::fmod(std::atan2(sinal, cosal) + 2. * M_PI, 2. * M_PI);
+     float smin = sst, smax = e->opts.spndr[1];
+     if (e->opts.allsky) {
+          smin = std::trunc((e->seg.Smin - nn * M[9] - mm * M[13]) / M[5]);
+          smax = std::trunc(-(nn * M[9] + mm * M[13] + e->seg.Smax) / M[5]);
+          if (smin > smax) {
+               smin = smin + smax;
+               smax = smin - smax;
+               smin = smin - smax;
+          }
+     }
+     float sstep = e->opts.sstep;
+     if (e->opts.allsky && !(sstep > 0)) sstep = 1.f;
+     P.smin = smin;
+     int iss = (int)((smax - smin) / sstep + 1);
+     P.iss_size = iss > 0 ? iss : 0;
+}
+
+static void tmpl_setup(const tdf_engine *e, const HostPoint &P, float mm, float nn, float ss, HostTmpl &T) {
+     const double *M = e->seg.M;
+     T.ss = ss;
+     T.spnd = ss * M[5] + nn * M[9] + mm * M[13];
+     double het1 = std::fmod(ss * M[4], M[0]);
+     if (het1 < 0) het1 += M[0];
+     T.het1 = het1;
+     if (e->form == TDF_FORM_SPLIT) {
+          // FLOAT build: het1 and sgnl0 are float (jobcore.c:458-468)
+          float h1 = (float)std::fmod(ss * M[4], M[0]);
+          if (h1 < 0) h1 += M[0];
+          float s0 = P.sp.het0 + h1;
+          T.sgnl0 = (double)s0;
+     } else {
+          T.sgnl0 = P.sp.het0 + het1;
+     }
+}
+
+// fdot of the record (jobcore.c:439,447): sgnlt[1] is FLOAT_TYPE
+static float rec_fdot(const tdf_engine *e, double spnd) {
+     if (e->form == TDF_FORM_SPLIT) return (float)((double)(float)spnd / (M_PI * e->seg.dt * e->seg.dt));
+     return (float)(spnd / (M_PI * e->seg.dt * e->seg.dt));
+}
+
+// ------------------------------------------------------------------ device pipeline
+
+static int run_sky_stage(tdf_engine *e, int npts) {
+     cudaStream_t st = e->stream;
+     const int nifo = e->nifo, Q = npts * nifo;
+     const size_t ws = Wstride(e);
+     CUCHK(cudaMemcpyAsync(e->skyp.p, e->h_sky, npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
+     const int nblk = e->nfft / 256;
+     const bool split = e->form == TDF_FORM_SPLIT;
+     k_sky_prep<<<dim3(nblk, Q), 256, 0, st>>>(
+          e->xdat.as<float>(), e->detssb.as<double>(), e->cosm.as<double>(), e->sinm.as<double>(),
+          e->skyp.as<SkyParam>(), e->detp.as<DetParam>(), nifo, e->N, e->nfft, e->Nal, e->seg.oms,
+          e->B0.as<double2>(), ws, e->shftf.as<double>(), split ? e->s2.as<float>() : nullptr,
+          split ? nullptr : e->t1.as<double>(), e->partial.as<double>());
+     CUCHK(cudaGetLastError());
+     k_sky_sums<<<(npts + 31) / 32, 32, 0, st>>>(e->partial.as<double>(), nblk, e->detp.as<DetParam>(), nifo, npts,
+                                                   e->aabb.as<AaBb>());
+     CUCHK(cudaGetLastError());
+     e->launches += 2;
+     // forward FFT (nfft) of every (point, detector, a|b): B0 -> B1 -> B2
+     {
+          const FFTTables<double> &t = e->t_nfft;
+          LoadNatural<double> pro{e->B0.as<double2>(), t.N2, (int)ws};
+          StoreFourstep<double, -1, 1> epi{e->B1.as<double2>(), t.h(), t.o(), t.N2, (int)ws};
+          TRY((launch_col<double, -1, 1>(t.N1, dim3(t.N2 / LINES, 2 * Q), pro, epi, t.l1(), st)));
+          RowsY<double, 1> src{e->B1.as<double2>(), (int)ws, t.N2};
+          StoreNatural<double> epi2{e->B2.as<double2>(), t.N1, (int)ws, e->nfft, 1.0};
+          TRY((launch_row<double, -1, 1>(t.N2, dim3(t.N1 / LINES, 2 * Q), src, epi2, t.l2(), st)));
+     }
+     // inverse FFT (Ninterp) of the spread spectrum, scaled by interpftpad/Ninterp:
+     // B2 -> B1 -> B0 (first interpftpad*N samples kept)
+     {
+          const FFTTables<double> &t = e->t_ninterp;
+          LoadShuffled<double> pro{e->B2.as<double2>(), t.N2, (int)ws, e->nfft, e->Ninterp};
+          StoreFourstep<double, +1, 1> epi{e->B1.as<double2>(), t.h(), t.o(), t.N2, (int)ws};
+          TRY((launch_col<double, +1, 1>(t.N1, dim3(t.N2 / LINES, 2 * Q), pro, epi, t.l1(), st)));
+          RowsY<double, 1> src{e->B1.as<double2>(), (int)ws, t.N2};
+          const double ft = (double)e->seg.interpftpad / e->Ninterp;
+          StoreNatural<double> epi2{e->B0.as<double2>(), t.N1, (int)ws, e->n2N, ft};
+          TRY((launch_row<double, +1, 1>(t.N2, dim3(t.N1 / LINES, 2 * Q), src, epi2, t.l2(), st)));
+     }
+     e->launches += 4;
+     // spline: B0 (samples) -> B1 (u) -> B2 (second derivatives)
+     {
+          const int K = 128, Wu = 48;
+          const int nch = (e->n2N + K - 1) / K;
+          dim3 g((nch + 127) / 128, 2 * Q);
+          k_spline_fwd<<<g, 128, 0, st>>>(e->B0.as<double2>(), e->B1.as<double2>(), ws, e->pco.as<double>(), e->n2N, K, Wu);
+          CUCHK(cudaGetLastError());
+          k_spline_bwd<<<g, 128, 0, st>>>(e->B1.as<double2>(), e->B2.as<double2>(), ws, e->gco.as<double>(), e->n2N, K, Wu);
+          CUCHK(cudaGetLastError());
+     }
+     k_splint<<<dim3((e->N + 255) / 256, Q), 256, 0, st>>>(
+          e->B0.as<double2>(), e->B2.as<double2>(), ws, e->shftf.as<double>(), e->Nal, e->N, e->n2N,
+          e->seg.interpftpad, e->detp.as<DetParam>(), nifo, split ? e->xab.as<float4>() : nullptr,
+          split ? nullptr : e->xa64.as<double2>(), split ? nullptr : e->xb64.as<double2>());
+     CUCHK(cudaGetLastError());
+     e->launches += 3;
+     return TDF_OK;
+}
+
+// spindown stage for templates [t0, t0+nt) of the staged parameter array
+template <typename T>
+static int run_chunk(tdf_engine *e, const TmplParam *dtp, int nt) {
+     cudaStream_t st = e->stream;
+     const bool split = std::is_same<T, float>::value;
+     const FFTTables<T> *tb;
+     if constexpr (std::is_same<T, float>::value) tb = &e->t_f32;
+     else tb = &e->t_f64;
+     const FFTTables<T> &t = *tb;
+     CUCHK(cudaMemsetAsync(e->tcnt.p, 0, nt * sizeof(unsigned), st));
+     StoreFourstep<T, -1, 2> epi{e->Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
+     size_t tev = e->timing ? timing_begin(e) : (size_t)-1;
+     if constexpr (std::is_same<T, float>::value) {
+          DemodSplit pro{e->xab.as<float4>(), e->s2.as<float>(), dtp, e->N, t.N2, e->Nal, e->nifo};
+          TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
+     } else {
+          DemodFP64 pro{e->xa64.as<double2>(), e->xb64.as<double2>(), e->t1.as<double>(), dtp, e->N, t.N2, e->Nal, e->nifo};
+          TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
+     }
+     if (e->timing) timing_end(e, tev, KT_COL, nt);
+     RowsY<T, 2> src{e->Ybuf.as<cx<T>>(), e->nfftf, t.N2};
+     StoreFstat<T> epi2{e->Fbuf.as<T>(), dtp, e->aabb.as<AaBb>(), e->nF, e->opts.fr[0], e->opts.fr[1], t.N1};
+     tev = e->timing ? timing_begin(e) : (size_t)-1;
+     TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+     if (e->timing) timing_end(e, tev, KT_ROW, nt);
+     e->launches += 2;
+     const T *mu = nullptr;
+     if (e->opts.blocks_avg && e->nblk_mu > 0) {
+          k_block_means<T><<<dim3(e->nblk_mu, nt), 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->nblk_mu, e->mubuf.as<T>());
+          CUCHK(cudaGetLastError());
+          mu = e->mubuf.as<T>();
+          e->launches++;
+     }
+     unsigned long long *cnt = e->counters.as<unsigned long long>();
+     dim3 g((e->nF + 255) / 256, nt);
+     tev = e->timing ? timing_begin(e) : (size_t)-1;
+     if (split)
+          k_threshold<T, false><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->opts.fr[0], e->opts.fr[1], e->opts.thr, mu,
+                                                    e->nblk_mu, dtp, e->nfftf, e->linesd.as<double>(), e->opts.numlines,
+                                                    (unsigned)(e->opts.bufsize / 2), e->trig.as<Trig>(), e->trig_cap, cnt,
+                                                    e->tcnt.as<unsigned>(), reinterpret_cast<unsigned *>(cnt + 1));
+     else
+          k_threshold<T, true><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->opts.fr[0], e->opts.fr[1], e->opts.thr, mu,
+                                                   e->nblk_mu, dtp, e->nfftf, e->linesd.as<double>(), e->opts.numlines,
+                                                   (unsigned)(e->opts.bufsize / 2), e->trig.as<Trig>(), e->trig_cap, cnt,
+                                                   e->tcnt.as<unsigned>(), reinterpret_cast<unsigned *>(cnt + 1));
+     CUCHK(cudaGetLastError());
+     if (e->timing) timing_end(e, tev, KT_THR, nt);
+     e->launches++;
+     return TDF_OK;
+}
+
+static int ensure_tparam(tdf_engine *e, size_t n) {
+     if (n > e->h_tp_cap) {
+          if (e->h_tp) {
+               CUCHK(cudaStreamSynchronize(e->stream));
+               cudaFreeHost(e->h_tp);
+               e->h_tp = nullptr;
+          }
+          size_t cap = std::max<size_t>(n, 4096);
+          CUCHK(cudaMallocHost((void **)&e->h_tp, cap * sizeof(TmplParam)));
+          e->h_tp_cap = cap;
+          TRY(e->tparam.alloc(cap * sizeof(TmplParam)));
+     }
+     return TDF_OK;
+}
+
+// The whole search over npts points.  Fills host-side templates (and
+// optionally collects triggers).  On return *ntrig_total holds the trigger
+// count; triggers are appended to e->h_trig when `collect`.
+static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn, const float *sst,
+                       std::vector<HostPoint> &pts, std::vector<HostTmpl> &tm, bool collect, int64_t *ntrig_total) {
+     if (npts < 0) return set_error(TDF_ERR_INVALID, "npts < 0");
+     if (npts > 0 && (!pm || !mm || !nn)) return set_error(TDF_ERR_INVALID, "null sky point arrays");
+     pts.assign(npts, HostPoint());
+     tm.clear();
+     for (int i = 0; i < npts; i++) {
+          if (pm[i] != 1 && pm[i] != 2) return set_error(TDF_ERR_INVALID, "pm[%d]=%d (must be 1 or 2)", i, pm[i]);
+          float s0 = sst ? sst[i] : e->opts.spndr[0];
+          point_setup(e, pm[i], mm[i], nn[i], s0, pts[i]);
+          if (!pts[i].inside) continue;
+          pts[i].first_tmpl = (int)tm.size();
+          for (int iss = 0; iss < pts[i].iss_size; iss++) {
+               HostTmpl T;
+               T.pt = i;
+               float ss = pts[i].smin + iss * e->opts.sstep;
+               tmpl_setup(e, pts[i], mm[i], nn[i], ss, T);
+               tm.push_back(T);
+          }
+     }
+     e->h_trig.clear();
+     *ntrig_total = 0;
+     unsigned long long *cnt = e->counters.as<unsigned long long>();
+     CUCHK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), e->stream));
+     // sky batches of consecutive inside points
+     std::vector<int> inside;
+     for (int i = 0; i < npts; i++)
+          if (pts[i].inside && pts[i].iss_size > 0) inside.push_back(i);
+     for (size_t b0 = 0; b0 < inside.size(); b0 += e->Bs) {
+          const int nb = (int)std::min<size_t>(e->Bs, inside.size() - b0);
+          CUCHK(cudaStreamSynchronize(e->stream));   // pinned staging reuse
+          int nt = 0;
+          for (int k = 0; k < nb; k++) {
+               const HostPoint &P = pts[inside[b0 + k]];
+               e->h_sky[k] = P.sp;
+               nt += P.iss_size;
+          }
+          TRY(ensure_tparam(e, nt));
+          int w = 0;
+          for (int k = 0; k < nb; k++) {
+               const HostPoint &P = pts[inside[b0 + k]];
+               for (int s = 0; s < P.iss_size; s++) {
+                    const HostTmpl &T = tm[P.first_tmpl + s];
+                    TmplParam &q = e->h_tp[w++];
+                    q.het1 = T.het1;
+                    q.spnd = T.spnd;
+                    q.sgnl0 = T.sgnl0;
+                    q.slot = k;
+                    q.id = (uint32_t)(P.first_tmpl + s);
+               }
+          }
+          size_t sev = e->timing ? timing_begin(e) : (size_t)-1;
+          TRY(run_sky_stage(e, nb));
+          if (e->timing) timing_end(e, sev, KT_SKY, nb);
+          CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp, nt * sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
+          for (int c0 = 0; c0 < nt; c0 += e->Tc) {
+               const int n = std::min(e->Tc, nt - c0);
+               if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, e->tparam.as<TmplParam>() + c0, n));
+               else TRY(run_chunk<double>(e, e->tparam.as<TmplParam>() + c0, n));
+          }
+          // drain this batch's triggers
+          CUCHK(cudaMemcpyAsync(e->h_cnt, cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
+          CUCHK(cudaStreamSynchronize(e->stream));
+          if (e->timing) timing_collect(e);
+          const unsigned long long nfound = e->h_cnt[0];
+          const unsigned errf = (unsigned)(e->h_cnt[1] & 0xffffffffu);
+          if (errf & ERR_OVERFLOW)
+               return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
+          if (nfound > e->trig_cap) {
+               // grow the trigger buffer and redo this batch's spindown stage
+               CUCHK(cudaStreamSynchronize(e->stream));
+               e->trig_cap = std::max<unsigned long long>(nfound + (nfound >> 2), e->trig_cap * 2);
+               e->trig.release();
+               TRY(e->trig.alloc(e->trig_cap * sizeof(Trig)));
+               CUCHK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), e->stream));
+               for (int c0 = 0; c0 < nt; c0 += e->Tc) {
+                    const int n = std::min(e->Tc, nt - c0);
+                    if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, e->tparam.as<TmplParam>() + c0, n));
+                    else TRY(run_chunk<double>(e, e->tparam.as<TmplParam>() + c0, n));
+               }
+               CUCHK(cudaMemcpyAsync(e->h_cnt, cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
+               CUCHK(cudaStreamSynchronize(e->stream));
+          }
+          const unsigned long long got = e->h_cnt[0];
+          *ntrig_total += (int64_t)got;
+          if (collect && got) {
+               size_t o = e->h_trig.size();
+               e->h_trig.resize(o + got);
+               CUCHK(cudaMemcpyAsync(e->h_trig.data() + o, e->trig.p, got * sizeof(Trig), cudaMemcpyDeviceToHost, e->stream));
+          }
+          CUCHK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), e->stream));
+     }
+     CUCHK(cudaStreamSynchronize(e->stream));
+     return TDF_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+const char *tdf_status_string(int status) {
+     switch (status) {
+     case TDF_OK: return "ok";
+     case TDF_ERR_INVALID: return "invalid argument";
+     case TDF_ERR_CUDA: return "CUDA error";
+     case TDF_ERR_TRIGGER_OVERFLOW: return "too many triggers in one spindown";
+     case TDF_ERR_OUT_OF_MEMORY: return "out of device memory";
+     case TDF_ERR_CAPACITY: return "output arrays too small";
+     case TDF_ERR_UNSUPPORTED: return "unsupported size or option";
+     case TDF_ERR_NO_DEVICE: return "no CUDA device";
+     case TDF_ERR_NOT_BUILT: return "not available in this build";
+     }
+     return "unknown status";
+}
+
+const char *tdf_last_error(void) { return g_last_error.c_str(); }
+
+int tdf_device_count(int *count) {
+     if (!count) return set_error(TDF_ERR_INVALID, "null count");
+     int n = 0;
+     cudaError_t e = cudaGetDeviceCount(&n);
+     if (e != cudaSuccess) {
+          *count = 0;
+          cudaGetLastError();
+          return set_error(TDF_ERR_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+     }
+     *count = n;
+     return TDF_OK;
+}
+
+int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int form, int device, int max_sky_batch,
+                      tdf_engine **out) {
+     if (!out) return set_error(TDF_ERR_INVALID, "null out");
+     *out = nullptr;
+     TRY(validate(seg, opts));
+     if (form != TDF_FORM_SPLIT && form != TDF_FORM_FP64) return set_error(TDF_ERR_INVALID, "form=%d", form);
+     if (form == TDF_FORM_FP64 && seg->nfftf > (1 << 18))
+          return set_error(TDF_ERR_UNSUPPORTED, "FP64 form supports nfftf <= 2^18");
+     int ndev = 0;
+     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+          cudaGetLastError();
+          return set_error(TDF_ERR_NO_DEVICE, "no CUDA device");
+     }
+     if (device < 0 || device >= ndev) return set_error(TDF_ERR_INVALID, "device %d of %d", device, ndev);
+     CUCHK(cudaSetDevice(device));
+     tdf_engine *e = new tdf_engine();
+     e->dev = device;
+     e->form = form;
+     e->seg = *seg;
+     e->opts = *opts;
+     e->N = seg->N;
+     e->nfft = seg->nfft;
+     e->nfftf = seg->nfftf;
+     e->Ninterp = seg->Ninterp;
+     e->nifo = seg->nifo;
+     e->Nal = (seg->N + 255) / 256 * 256;
+     e->n2N = seg->interpftpad * seg->N;
+     e->nF = opts->fr[1] - opts->fr[0] + 1;
+     e->nblk_mu = opts->blocks_avg ? (opts->fr[1] - opts->fr[0]) / TDF_NAVFSTAT : 0;
+     if (max_sky_batch > 0) e->Bs = max_sky_batch;
+     const char *tc = getenv("TDF_TEMPLATES_PER_CHUNK");
+     if (tc && atoi(tc) > 0) e->Tc = atoi(tc);
+     e->lines.assign(opts->lines, opts->lines + 2 * (size_t)opts->numlines);
+     e->opts.lines = nullptr;
+     e->dets.resize(seg->nifo);
+     int st = TDF_OK;
+     cudaError_t ce = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking);
+     if (ce != cudaSuccess) st = set_error(TDF_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce));
+     e->stream = e->own;
+     if (st == TDF_OK) st = engine_alloc(e);
+     if (st == TDF_OK) st = upload_inputs(e, seg);
+     if (st == TDF_OK) {
+          ce = cudaStreamSynchronize(e->stream);
+          if (ce != cudaSuccess) st = set_error(TDF_ERR_CUDA, "upload: %s", cudaGetErrorString(ce));
+     }
+     if (st != TDF_OK) {
+          engine_free(e);
+          delete e;
+          return st;
+     }
+     *out = e;
+     return TDF_OK;
+}
+
+int tdf_engine_upload(tdf_engine *e, const tdf_segment *seg) {
+     if (!e || !seg) return set_error(TDF_ERR_INVALID, "null engine or segment");
+     tdf_search_opts o = e->opts;
+     o.lines = e->lines.data();
+     TRY(validate(seg, &o));
+     if (seg->N != e->N || seg->nfft != e->nfft || seg->nfftf != e->nfftf || seg->Ninterp != e->Ninterp ||
+         seg->nifo != e->nifo)
+          return set_error(TDF_ERR_INVALID, "segment sizes differ from the engine's");
+     CUCHK(cudaSetDevice(e->dev));
+     TRY(upload_inputs(e, seg));
+     return TDF_OK;
+}
+
+int tdf_engine_destroy(tdf_engine *e) {
+     if (!e) return TDF_OK;
+     cudaSetDevice(e->dev);
+     if (e->stream) cudaStreamSynchronize(e->stream);
+     engine_free(e);
+     delete e;
+     return TDF_OK;
+}
+
+int tdf_search_points(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn, const float *sst,
+                      tdf_record *recs, int64_t max_recs, int64_t *nrec, float *pairs, int64_t max_pairs,
+                      int64_t *npairs, int32_t *nrec_per_point) {
+     if (!e || !nrec || !npairs) return set_error(TDF_ERR_INVALID, "null engine or count pointers");
+     CUCHK(cudaSetDevice(e->dev));
+     std::vector<HostPoint> pts;
+     std::vector<HostTmpl> tm;
+     int64_t ntrig = 0;
+     TRY(search_core(e, npts, pm, mm, nn, sst, pts, tm, true, &ntrig));
+     // sort triggers into (template, bin) order: the reference's order
+     std::vector<Trig> &tg = e->h_trig;
+     std::sort(tg.begin(), tg.end(), [](const Trig &a, const Trig &b) {
+          return a.id != b.id ? a.id < b.id : a.bin < b.bin;
+     });
+     const int64_t need_recs = (int64_t)tm.size(), need_pairs = 2 * (int64_t)tg.size();
+     *nrec = need_recs;
+     *npairs = need_pairs;
+     if (nrec_per_point)
+          for (int i = 0; i < npts; i++) nrec_per_point[i] = pts[i].inside ? pts[i].iss_size : 0;
+     if (need_recs > max_recs || need_pairs > max_pairs || (need_recs && !recs) || (need_pairs && !pairs))
+          return set_error(TDF_ERR_CAPACITY, "need %lld records and %lld floats", (long long)need_recs,
+                           (long long)need_pairs);
+     size_t k = 0;
+     int64_t off = 0;
+     for (size_t t = 0; t < tm.size(); t++) {
+          const HostTmpl &T = tm[t];
+          const HostPoint &P = pts[T.pt];
+          tdf_record &r = recs[t];
+          r.m = mm[T.pt];
+          r.n = nn[T.pt];
+          r.s = T.ss;
+          r.ra = P.ra;
+          r.dec = P.dec;
+          r.fdot = rec_fdot(e, T.spnd);
+          r.pad = 0;
+          r.offset = off;
+          uint32_t len = 0;
+          while (k < tg.size() && tg[k].id == (uint32_t)t) {
+               pairs[off++] = tg[k].f;
+               pairs[off++] = tg[k].F;
+               len += 2;
+               k++;
+          }
+          r.len = len;
+     }
+     return TDF_OK;
+}
+
+int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
+                             const float *sst, int64_t *nrec, int64_t *ntrig) {
+     if (!e || !nrec || !ntrig) return set_error(TDF_ERR_INVALID, "null engine or count pointers");
+     CUCHK(cudaSetDevice(e->dev));
+     std::vector<HostPoint> pts;
+     std::vector<HostTmpl> tm;
+     TRY(search_core(e, npts, pm, mm, nn, sst, pts, tm, false, ntrig));
+     *nrec = (int64_t)tm.size();
+     return TDF_OK;
+}
+
+int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, double *F, int64_t nF) {
+     if (!e || !F) return set_error(TDF_ERR_INVALID, "null engine or output");
+     if (nF < e->nF) return set_error(TDF_ERR_CAPACITY, "need %d values", e->nF);
+     if (pm != 1 && pm != 2) return set_error(TDF_ERR_INVALID, "pm=%d", pm);
+     CUCHK(cudaSetDevice(e->dev));
+     HostPoint P;
+     point_setup(e, pm, mm, nn, e->opts.spndr[0], P);
+     if (!P.inside) return set_error(TDF_ERR_INVALID, "sky point outside the grid ellipse");
+     HostTmpl T;
+     tmpl_setup(e, P, mm, nn, ss, T);
+     CUCHK(cudaStreamSynchronize(e->stream));
+     e->h_sky[0] = P.sp;
+     TRY(ensure_tparam(e, 1));
+     TmplParam &q = e->h_tp[0];
+     q.het1 = T.het1;
+     q.spnd = T.spnd;
+     q.sgnl0 = T.sgnl0;
+     q.slot = 0;
+     q.id = 0;
+     TRY(run_sky_stage(e, 1));
+     CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp, sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
+     CUCHK(cudaMemsetAsync(e->counters.p, 0, 2 * sizeof(unsigned long long), e->stream));
+     if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, e->tparam.as<TmplParam>(), 1));
+     else TRY(run_chunk<double>(e, e->tparam.as<TmplParam>(), 1));
+     const int n = e->nF;
+     if (e->form == TDF_FORM_SPLIT) {
+          std::vector<float> f(n), mu(std::max(1, e->nblk_mu));
+          CUCHK(cudaMemcpyAsync(f.data(), e->Fbuf.p, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+          if (e->nblk_mu)
+               CUCHK(cudaMemcpyAsync(mu.data(), e->mubuf.p, e->nblk_mu * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+          CUCHK(cudaStreamSynchronize(e->stream));
+          for (int i = 0; i < n; i++) F[i] = (i < e->nblk_mu * TDF_NAVFSTAT) ? (double)(f[i] / mu[i >> 12]) : (double)f[i];
+     } else {
+          std::vector<double> mu(std::max(1, e->nblk_mu));
+          CUCHK(cudaMemcpyAsync(F, e->Fbuf.p, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+          if (e->nblk_mu)
+               CUCHK(cudaMemcpyAsync(mu.data(), e->mubuf.p, e->nblk_mu * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+          CUCHK(cudaStreamSynchronize(e->stream));
+          for (int i = 0; i < n && i < e->nblk_mu * TDF_NAVFSTAT; i++) F[i] = F[i] / mu[i >> 12];
+     }
+     return TDF_OK;
+}
+
+int tdf_engine_get_stream(tdf_engine *e, void **stream) {
+     if (!e || !stream) return set_error(TDF_ERR_INVALID, "null argument");
+     *stream = (void *)e->stream;
+     return TDF_OK;
+}
+
+int tdf_engine_set_stream(tdf_engine *e, void *stream) {
+     if (!e) return set_error(TDF_ERR_INVALID, "null engine");
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     e->stream = stream ? (cudaStream_t)stream : e->own;
+     return TDF_OK;
+}
+
+int tdf_engine_launch_count(tdf_engine *e, int64_t *count) {
+     if (!e || !count) return set_error(TDF_ERR_INVALID, "null argument");
+     *count = e->launches;
+     return TDF_OK;
+}
+
+int tdf_engine_set_kernel_timing(tdf_engine *e, int on) {
+     if (!e) return set_error(TDF_ERR_INVALID, "null engine");
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     if (e->timing) timing_collect(e);
+     e->timing = on != 0;
+     if (on) e->kt = tdf_kernel_times{};
+     return TDF_OK;
+}
+
+int tdf_engine_get_kernel_times(tdf_engine *e, tdf_kernel_times *out) {
+     if (!e || !out) return set_error(TDF_ERR_INVALID, "null argument");
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     timing_collect(e);
+     *out = e->kt;
+     return TDF_OK;
+}
+
+}  // extern "C"

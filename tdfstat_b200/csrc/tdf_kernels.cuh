@@ -1,0 +1,464 @@
+// tdf_kernels.cuh -- the hot-path kernels of the job_core() chain
+// (search/network/openmp/jobcore.c:193-630) other than the FFT passes:
+//
+//   sky stage (FP64, once per sky point and detector)
+//     k_sky_prep      modvir + barycentric shift + phase modulation
+//                     (settings.c:254-294, jobcore.c:283-312), zero padding,
+//                     partial sums of aa^2, bb^2 (jobcore.c:373-391)
+//     k_sky_sums      aa, bb network sums (FLOAT_TYPE emulation per form)
+//     k_spline_fwd /
+//     k_spline_bwd    natural cubic spline second derivatives (auxi.c:93-117)
+//                     as blocked recurrences with warm-up
+//     k_splint        spline evaluation at 2(i - shftf[i]) (auxi.c:120-169),
+//                     division by sig2, conversion to the spindown operands
+//   spindown stage (once per template)
+//     DemodSplit /
+//     DemodFP64       column-pass prologues: spindown_modulation
+//                     (spinmod.c:490-514) fused into the first FFT pass
+//     StoreFstat      row-pass epilogue: F = |Fa|^2/aa + |Fb|^2/bb
+//                     (jobcore.c:481-484)
+//     k_block_means   FStat blocks_avg means (auxi.c:336-363)
+//     k_threshold     MAX_ALG 3 local maxima, veto, trigger append
+//                     (jobcore.c:552-603)
+#pragma once
+
+#include <float.h>
+#include "tdf_passes.cuh"
+
+namespace tdf {
+
+struct SkyParam {
+     double sinalt, cosalt, sindelt, cosdelt, het0;
+     double nS0, nS1, nS2;
+};
+
+struct DetParam {
+     double amod[9];
+     double cphir, sphir, sig2;
+};
+
+// one template: (sky slot, spindown)
+struct TmplParam {
+     double het1;     // fmod(ss*M[4], M[0]) (+M[0] if negative), FP64
+     double spnd;     // ss*M[5] + nn*M[9] + mm*M[13], FP64
+     double sgnl0;    // het0 + het1 as the emulated build rounds it (trigger frequency)
+     int32_t slot;    // operand slot of the sky point
+     uint32_t id;     // template number within the call
+};
+
+struct AaBb {
+     double aa, bb;
+     float aaf, bbf;
+};
+
+struct Trig {
+     uint32_t id, bin;
+     float f, F;
+};
+
+constexpr unsigned ERR_OVERFLOW = 1u;
+constexpr double TWO_PI = 6.283185307179586476925286766559;
+constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
+constexpr double M_PI_D = 3.14159265358979323846;
+
+// ------------------------------------------------------------------ sky stage
+
+// grid (ceil(nfft/256), Q = npts*nifo), 256 threads
+__global__ void __launch_bounds__(256) k_sky_prep(
+     const float *__restrict__ xdat, const double *__restrict__ detssb,
+     const double *__restrict__ cosm, const double *__restrict__ sinm,
+     const SkyParam *__restrict__ sp, const DetParam *__restrict__ dp,
+     int nifo, int N, int nfft, int Nal, double oms,
+     double2 *__restrict__ W, size_t Wstride, double *__restrict__ shftf,
+     float *__restrict__ s2, double *__restrict__ t1, double *__restrict__ partial)
+{
+     const int q = blockIdx.y, p = q / nifo, d = q % nifo;
+     const int i = blockIdx.x * 256 + threadIdx.x;
+     double a2 = 0., b2 = 0.;
+     if (i < nfft) {
+          double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
+          if (i < N) {
+               const SkyParam S = sp[p];
+               const DetParam &D = dp[d];
+               const float x = xdat[(size_t)d * Nal + i];
+               double aa = 0., bb = 0.;
+               if (fabs((double)x) > DBL_MIN) {
+                    const double cosalfr = S.cosalt * D.cphir + S.sinalt * D.sphir;
+                    const double sinalfr = S.sinalt * D.cphir - S.cosalt * D.sphir;
+                    const double c2d = S.cosdelt * S.cosdelt, c2sd = S.sindelt * S.cosdelt;
+                    const double c = cosalfr * cosm[i] + sinalfr * sinm[i];
+                    const double s = sinalfr * cosm[i] - cosalfr * sinm[i];
+                    const double c2s = 2. * c * c, cs = c * s;
+                    aa = D.amod[0] * (2. - c2d) * c2s + D.amod[1] * (2. - c2d) * 2. * cs +
+                         D.amod[2] * c2sd * c + D.amod[3] * c2sd * s - D.amod[0] * (2. - c2d) + D.amod[4] * c2d;
+                    bb = D.amod[5] * S.sindelt * c2s + D.amod[6] * S.sindelt * 2. * cs +
+                         D.amod[7] * S.cosdelt * c + D.amod[8] * S.cosdelt * s - D.amod[5] * S.sindelt;
+               }
+               const double *e = detssb + (size_t)d * 3 * N;
+               // shift and phase without FMA contraction: the phase reaches
+               // ~1e5 rad, so its rounding must follow the reference's
+               const double sh = __dadd_rn(__dadd_rn(__dmul_rn(S.nS0, e[3 * (size_t)i]), __dmul_rn(S.nS1, e[3 * (size_t)i + 1])),
+                                           __dmul_rn(S.nS2, e[3 * (size_t)i + 2]));
+               const double sh1 = __dadd_rn(__dadd_rn(__dmul_rn(S.nS0, e[0]), __dmul_rn(S.nS1, e[1])), __dmul_rn(S.nS2, e[2]));
+               shftf[(size_t)q * Nal + i] = __dsub_rn(sh, sh1);
+               const size_t o = ((size_t)p * nifo + d) * Nal + i;
+               const double di = (double)i;
+               if (s2) s2[o] = (float)__dmul_rn((double)(2 * i), sh);
+               if (t1) t1[o] = __dadd_rn(__dmul_rn(di, di), __dmul_rn((double)(2 * i), sh));
+               const double phase = __dadd_rn(__dmul_rn(S.het0, di), __dmul_rn(oms, sh));
+               double sn, cn;
+               sincos(phase, &sn, &cn);
+               const double ra = (double)x * aa, rb = (double)x * bb;
+               xa = make_double2(ra * cn, ra * -sn);
+               xb = make_double2(rb * cn, rb * -sn);
+               a2 = aa * aa;
+               b2 = bb * bb;
+          }
+          W[((size_t)q * 2 + 0) * Wstride + i] = xa;
+          W[((size_t)q * 2 + 1) * Wstride + i] = xb;
+     }
+     // block partial sums of aa^2, bb^2
+     __shared__ double ra_[8], rb_[8];
+#pragma unroll
+     for (int o = 16; o > 0; o >>= 1) {
+          a2 += __shfl_down_sync(0xffffffffu, a2, o);
+          b2 += __shfl_down_sync(0xffffffffu, b2, o);
+     }
+     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+     if (l == 0) { ra_[w] = a2; rb_[w] = b2; }
+     __syncthreads();
+     if (threadIdx.x == 0) {
+          double sa = 0., sb = 0.;
+          for (int k = 0; k < 8; k++) { sa += ra_[k]; sb += rb_[k]; }
+          partial[((size_t)q * gridDim.x + blockIdx.x) * 2 + 0] = sa;
+          partial[((size_t)q * gridDim.x + blockIdx.x) * 2 + 1] = sb;
+     }
+}
+
+// one thread per sky point: aa = sum_n sum_i aa_n^2/sig2_n (jobcore.c:373-386),
+// accumulated per detector into FLOAT_TYPE as the reference build does
+__global__ void k_sky_sums(const double *__restrict__ partial, int nblk, const DetParam *__restrict__ dp,
+                           int nifo, int npts, AaBb *__restrict__ out)
+{
+     const int p = blockIdx.x * blockDim.x + threadIdx.x;
+     if (p >= npts) return;
+     double aa = 0., bb = 0.;
+     float aaf = 0.f, bbf = 0.f;
+     for (int d = 0; d < nifo; d++) {
+          const double *pp = partial + (size_t)(p * nifo + d) * nblk * 2;
+          double sa = 0., sb = 0.;
+          for (int k = 0; k < nblk; k++) { sa += pp[2 * k]; sb += pp[2 * k + 1]; }
+          aa += sa / dp[d].sig2;
+          bb += sb / dp[d].sig2;
+          aaf = (float)((double)aaf + sa / dp[d].sig2);
+          bbf = (float)((double)bbf + sb / dp[d].sig2);
+     }
+     out[p].aa = aa;
+     out[p].bb = bb;
+     out[p].aaf = aaf;
+     out[p].bbf = bbf;
+}
+
+// Forward sweep of the natural spline (auxi.c:102-111), u[i] for i in [1, n-2]
+// (u[0] = 0).  Thread = chunk of K indices, started W indices early from
+// u = 0: the recurrence contracts by |0.5*invp| ~ 0.27 per step, so the
+// start-up error is below 1e-27 of |u| after W = 48 steps.
+// grid (ceil(nchunk/128), 2*Q), 128 threads
+__global__ void k_spline_fwd(const double2 *__restrict__ Z, double2 *__restrict__ U, size_t stride,
+                             const double *__restrict__ pco, int n, int K, int Wu)
+{
+     const int arr = blockIdx.y;
+     const int c = blockIdx.x * blockDim.x + threadIdx.x;
+     const int lo = c * K;
+     if (lo >= n) return;
+     const double2 *y = Z + (size_t)arr * stride;
+     double2 *u = U + (size_t)arr * stride;
+     const int hi = min(n - 1, lo + K);
+     if (lo == 0) u[0] = make_double2(0., 0.);
+     int i0 = max(1, lo - Wu);
+     double ur = 0., ui = 0.;
+     double2 ym = y[i0 - 1], y0 = y[i0];
+     for (int i = i0; i < hi; i++) {
+          const double2 yp = y[i + 1];
+          const double p = pco[i];
+          const double dr = ym.x - 2. * y0.x + yp.x;
+          const double dI = ym.y - 2. * y0.y + yp.y;
+          ur = (-.5 * ur + 3. * dr) * p;
+          ui = (-.5 * ui + 3. * dI) * p;
+          if (i >= lo) u[i] = make_double2(ur, ui);
+          ym = y0;
+          y0 = yp;
+     }
+}
+
+// Back substitution (auxi.c:112-115): y2[n-1] = 0, y2[k] = g[k]*y2[k+1] + u[k].
+// Thread = chunk of K indices, started W indices late from y2 = 0.
+__global__ void k_spline_bwd(const double2 *__restrict__ U, double2 *__restrict__ Y2, size_t stride,
+                             const double *__restrict__ gco, int n, int K, int Wu)
+{
+     const int arr = blockIdx.y;
+     const int c = blockIdx.x * blockDim.x + threadIdx.x;
+     const int lo = c * K;
+     if (lo >= n) return;
+     const double2 *u = U + (size_t)arr * stride;
+     double2 *y2 = Y2 + (size_t)arr * stride;
+     const int hi = min(n, lo + K);
+     const int ks = min(n - 1, hi + Wu);
+     if (ks == n - 1 && ks < hi) y2[n - 1] = make_double2(0., 0.);
+     double yr = 0., yi = 0.;
+     for (int k = ks - 1; k >= lo; k--) {
+          const double g = gco[k];
+          const double2 uk = u[k];
+          yr = g * yr + uk.x;
+          yi = g * yi + uk.y;
+          if (k < hi) y2[k] = make_double2(yr, yi);
+     }
+}
+
+__device__ __forceinline__ double2 splint_eval(const double2 *__restrict__ ya, const double2 *__restrict__ y2a, int n, double x)
+{
+     if (x < 0 || x > n - 1) return make_double2(0., 0.);
+     const int klo = (int)floor(x);
+     const int khi = klo + 1;
+     const double a = khi - x, b = x - klo;
+     const double2 yl = ya[klo], sl = y2a[klo];
+     const double2 yh = khi < n ? ya[khi] : make_double2(0., 0.);
+     const double2 sh = khi < n ? y2a[khi] : make_double2(0., 0.);
+     const double ca = a * a * a - a, cb = b * b * b - b;
+     return make_double2(a * yl.x + b * yh.x + (ca * sl.x + cb * sh.x) / 6.0,
+                         a * yl.y + b * yh.y + (ca * sl.y + cb * sh.y) / 6.0);
+}
+
+// grid (ceil(N/256), Q), 256 threads: xDatm{a,b}[i] = splint(...)/sig2 as
+// split (float4 xa.re, xa.im, xb.re, xb.im) or FP64 (two double2) operands
+__global__ void __launch_bounds__(256) k_splint(
+     const double2 *__restrict__ Z, const double2 *__restrict__ Y2, size_t stride,
+     const double *__restrict__ shftf, int Nal, int N, int n, int interpftpad,
+     const DetParam *__restrict__ dp, int nifo,
+     float4 *__restrict__ xab, double2 *__restrict__ xa64, double2 *__restrict__ xb64)
+{
+     const int q = blockIdx.y, p = q / nifo, d = q % nifo;
+     const int i = blockIdx.x * 256 + threadIdx.x;
+     if (i >= N) return;
+     const double x = interpftpad * (i - shftf[(size_t)q * Nal + i]);
+     const double2 va = splint_eval(Z + ((size_t)q * 2) * stride, Y2 + ((size_t)q * 2) * stride, n, x);
+     const double2 vb = splint_eval(Z + ((size_t)q * 2 + 1) * stride, Y2 + ((size_t)q * 2 + 1) * stride, n, x);
+     const double s2 = dp[d].sig2;
+     const double2 a = make_double2(va.x / s2, va.y / s2), b = make_double2(vb.x / s2, vb.y / s2);
+     const size_t o = ((size_t)p * nifo + d) * Nal + i;
+     if (xab) xab[o] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+     if (xa64) { xa64[o] = a; xb64[o] = b; }
+}
+
+// ------------------------------------------------------------------ spindown stage
+
+// Neumaier-compensated accumulation of the detector-network sum
+struct CompSum {
+     float s, c;
+     __device__ __forceinline__ void init(float v) { s = v; c = 0.f; }
+     __device__ __forceinline__ void add(float x) {
+          float t = s + x;
+          c += (fabsf(s) >= fabsf(x)) ? ((s - t) + x) : ((x - t) + s);
+          s = t;
+     }
+     __device__ __forceinline__ float value() const { return s + c; }
+};
+
+// Split form: phase = het1*i + spnd*i^2 formed and reduced mod 2 pi in FP64,
+// plus spnd*(2 i shft_n[i]) in FP32 per detector; FP32 sincos and products,
+// compensated sum over detectors.
+struct DemodSplit {
+     const float4 *xab;
+     const float *s2;
+     const TmplParam *tp;
+     int N, N2, Nal, nifo;
+     template <int L>
+     __device__ __forceinline__ void load(float2 (&v)[2][8], int b, int n2, int t) const {
+          const TmplParam P = tp[b];
+          const float spf = (float)P.spnd;
+          const size_t base = (size_t)P.slot * nifo * Nal;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               const int i = N2 * (t + m * (L / 8)) + n2;
+               float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
+               if (i < N) {
+                    const double di = (double)i;
+                    const double ph = fma(P.spnd, di * di, P.het1 * di);
+                    const double kk = rint(ph * INV_TWO_PI);
+                    const float pr = (float)fma(-kk, TWO_PI, ph);
+                    CompSum ar, ai, br, bi;
+                    for (int d = 0; d < nifo; d++) {
+                         const size_t o = base + (size_t)d * Nal + i;
+                         const float4 x = __ldg(&xab[o]);
+                         const float phf = fmaf(spf, __ldg(&s2[o]), pr);
+                         float sn, cs;
+                         __sincosf(phf, &sn, &cs);
+                         // (x.re + i x.im) * (cs - i sn)
+                         const float pr_ = fmaf(x.x, cs, x.y * sn), pi_ = fmaf(x.y, cs, -x.x * sn);
+                         const float qr_ = fmaf(x.z, cs, x.w * sn), qi_ = fmaf(x.w, cs, -x.z * sn);
+                         if (d == 0) { ar.init(pr_); ai.init(pi_); br.init(qr_); bi.init(qi_); }
+                         else { ar.add(pr_); ai.add(pi_); br.add(qr_); bi.add(qi_); }
+                    }
+                    fa = make_float2(ar.value(), ai.value());
+                    fb = make_float2(br.value(), bi.value());
+               }
+               v[0][m] = fa;
+               v[1][m] = fb;
+          }
+     }
+};
+
+// Plain FP64 form: the reference's DOUBLE-build spindown_modulation.
+struct DemodFP64 {
+     const double2 *xa, *xb;
+     const double *t1;
+     const TmplParam *tp;
+     int N, N2, Nal, nifo;
+     template <int L>
+     __device__ __forceinline__ void load(double2 (&v)[2][8], int b, int n2, int t) const {
+          const TmplParam P = tp[b];
+          const size_t base = (size_t)P.slot * nifo * Nal;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               const int i = N2 * (t + m * (L / 8)) + n2;
+               double2 fa = make_double2(0., 0.), fb = make_double2(0., 0.);
+               if (i < N) {
+                    for (int d = 0; d < nifo; d++) {
+                         const size_t o = base + (size_t)d * Nal + i;
+                         const double phase = __dadd_rn(__dmul_rn(P.het1, (double)i), __dmul_rn(P.spnd, __ldg(&t1[o])));
+                         double sn, cs;
+                         sincos(phase, &sn, &cs);
+                         const double2 x = __ldg(&xa[o]), y = __ldg(&xb[o]);
+                         const double er = cs, ei = -sn;
+                         fa.x += x.x * er - x.y * ei;
+                         fa.y += x.x * ei + x.y * er;
+                         fb.x += y.x * er - y.y * ei;
+                         fb.y += y.x * ei + y.y * er;
+                    }
+               }
+               v[0][m] = fa;
+               v[1][m] = fb;
+          }
+     }
+};
+
+template <typename T> __device__ __forceinline__ T aa_of(const AaBb &ab);
+template <> __device__ __forceinline__ float aa_of<float>(const AaBb &ab) { return ab.aaf; }
+template <> __device__ __forceinline__ double aa_of<double>(const AaBb &ab) { return ab.aa; }
+template <typename T> __device__ __forceinline__ T bb_of(const AaBb &ab);
+template <> __device__ __forceinline__ float bb_of<float>(const AaBb &ab) { return ab.bbf; }
+template <> __device__ __forceinline__ double bb_of<double>(const AaBb &ab) { return ab.bb; }
+
+// Row-pass epilogue of the spindown FFT: F[k] over [fr0, fr1]
+template <typename T>
+struct StoreFstat {
+     T *F;
+     const TmplParam *tp;
+     const AaBb *ab;
+     int nF, fr0, fr1, N1;
+     template <int L>
+     __device__ __forceinline__ void store(const cx<T> (&v)[2][8], int b, int k1, int t) const {
+          const AaBb s = ab[tp[b].slot];
+          const T aa = aa_of<T>(s), bb = bb_of<T>(s);
+          T *dst = F + (size_t)b * nF - fr0;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               const int k = k1 + N1 * (t + m * (L / 8));
+               if (k >= fr0 && k <= fr1) dst[k] = cnorm(v[0][m]) / aa + cnorm(v[1][m]) / bb;
+          }
+     }
+};
+
+// blocks_avg means (auxi.c:349-355): mu_j = sum of the j-th block of NAV
+// values of F[fr0..] / (2 NAV).  grid (nblk, ntmpl), 256 threads
+template <typename T>
+__global__ void k_block_means(const T *__restrict__ F, int nF, int nblk, T *__restrict__ mu)
+{
+     const int j = blockIdx.x, b = blockIdx.y;
+     const T *src = F + (size_t)b * nF + (size_t)j * 4096;
+     T s = 0;
+     for (int k = threadIdx.x; k < 4096; k += 256) s += src[k];
+     __shared__ T red[256];
+     red[threadIdx.x] = s;
+     __syncthreads();
+     for (int o = 128; o > 0; o >>= 1) {
+          if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+          __syncthreads();
+     }
+     if (threadIdx.x == 0) mu[(size_t)b * nblk + j] = (T)(red[0] / (2. * 4096));
+}
+
+template <typename T>
+__device__ __forceinline__ T fval(const T *Fb, const T *mub, int k, int fr0, int nblk) {
+     T f = Fb[k];
+     if (mub) {
+          const int r = k - fr0;
+          if (r < nblk * 4096) f = f / mub[r >> 12];
+     }
+     return f;
+}
+
+template <typename T>
+__device__ __forceinline__ bool is_peak(const T *Fb, const T *mub, int k, int fr0, int nblk, double thr) {
+     const T f = fval(Fb, mub, k, fr0, nblk);
+     return !(f < thr || fval(Fb, mub, k - 1, fr0, nblk) > f || f < fval(Fb, mub, k + 1, fr0, nblk));
+}
+
+// MAX_ALG 3 (jobcore.c:556-603) as the single-threaded loop executes it:
+// bin i (fr0 < i < fr1-1) is a trigger when it is a local maximum >= thr
+// and the previous accepted bin is not i-1 (the loop's "i++" skip), i.e.
+// when the run of consecutive local-maximum bins ending at i-1 has even
+// length.  Then the veto intervals are checked and the trigger appended.
+// grid (ceil((fr1-fr0+1)/256), ntmpl), 256 threads
+template <typename T, bool FP64>
+__global__ void __launch_bounds__(256) k_threshold(
+     const T *__restrict__ F, int nF, int fr0, int fr1, double thr,
+     const T *__restrict__ mu, int nblk, const TmplParam *__restrict__ tp, int nfftf,
+     const double *__restrict__ lines, int numlines, unsigned bufhalf,
+     Trig *__restrict__ trig, unsigned long long cap, unsigned long long *cnt,
+     unsigned *__restrict__ tcnt, unsigned *err)
+{
+     const int b = blockIdx.y;
+     const int i = fr0 + blockIdx.x * 256 + threadIdx.x;
+     if (i < fr0 + 1 || i >= fr1 - 1) return;
+     const T *Fb = F + (size_t)b * nF - fr0;
+     const T *mub = mu ? mu + (size_t)b * nblk : nullptr;
+     if (!is_peak(Fb, mub, i, fr0, nblk, thr)) return;
+     int run = 0;
+     for (int k = i - 1; k >= fr0 + 1 && is_peak(Fb, mub, k, fr0, nblk, thr); k--) run++;
+     if (run & 1) return;
+     const T Fc = fval(Fb, mub, i, fr0, nblk);
+     const TmplParam P = tp[b];
+     double fcmp;
+     float ff;
+     if (FP64) {
+          // FLOAT_TYPE = double: f_ = (double)(2ic)/(double)nfftf*M_PI + sgnl0
+          const double f_ = __dadd_rn(__dmul_rn(__ddiv_rn((double)(2 * i), (double)nfftf), M_PI_D), P.sgnl0);
+          fcmp = f_;
+          ff = (float)f_;
+     } else {
+          // FLOAT_TYPE = float: the quotient in float, the product and sum in
+          // double, stored to float
+          const float qf = __fdiv_rn((float)(2 * i), (float)nfftf);
+          ff = (float)__dadd_rn(__dmul_rn((double)qf, M_PI_D), P.sgnl0);
+          fcmp = (double)ff;
+     }
+     for (int k = 0; k < numlines; k++)
+          if (fcmp >= lines[2 * k] && fcmp <= lines[2 * k + 1]) return;
+     const unsigned c = atomicAdd(&tcnt[b], 1u);
+     if (c >= bufhalf) {
+          atomicOr(err, ERR_OVERFLOW);
+          return;
+     }
+     const unsigned long long g = atomicAdd(cnt, 1ull);
+     if (g < cap) {
+          Trig r;
+          r.id = P.id;
+          r.bin = (uint32_t)i;
+          r.f = ff;
+          r.F = (float)Fc;
+          trig[g] = r;
+     }
+}
+
+}  // namespace tdf

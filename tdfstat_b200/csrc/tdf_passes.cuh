@@ -1,0 +1,175 @@
+// tdf_passes.cuh -- the two four-step pass kernels (see tdf_fft.cuh) and the
+// prologue/epilogue policies fused into them.
+//
+//   k_colpass<T, L, SIGN, NA, Pro, Epi>: CTA = LINES columns n2 of an
+//     N = L*N2 transform, L threads; Pro::load fills the first-pass inputs
+//     x[N2*n1 + n2] straight into registers (coalesced across the 8 columns),
+//     Epi::store consumes the outputs k1 = t + m*L/8.
+//   k_rowpass<T, L, SIGN, NA, Src, Epi>: CTA = LINES rows k1 of an
+//     N = N1*L transform, L threads; the rows are staged through shared
+//     memory with coalesced loads, Epi::store consumes X[k1 + N1*k2].
+#pragma once
+
+#include "tdf_fft.cuh"
+
+namespace tdf {
+
+template <typename T, int L, int NA>
+constexpr size_t pass_smem_bytes() {
+     return sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
+}
+
+template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
+__global__ void __launch_bounds__(L) k_colpass(Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
+     using G = LineGeom<T, L>;
+     extern __shared__ __align__(16) unsigned char smem_raw[];
+     cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
+     cx<T> *lines = tw + L;
+     load_table<T>(tw, twline, L);
+     const int tid = threadIdx.x;
+     const int c = tid % LINES, t = tid / LINES;
+     const int n2 = blockIdx.x * LINES + c;
+     const int b = blockIdx.y;
+     cx<T> v[NA][8];
+     pro.template load<L>(v, b, n2, t);
+     cx<T> *s[NA];
+#pragma unroll
+     for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
+     __syncthreads();
+     line_fft<T, L, SIGN, NA>(v, s, tw, t);
+     epi.template store<L>(v, b, n2, t);
+}
+
+template <typename T, int L, int SIGN, int NA, class Src, class Epi>
+__global__ void __launch_bounds__(L) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
+     using G = LineGeom<T, L>;
+     extern __shared__ __align__(16) unsigned char smem_raw[];
+     cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
+     cx<T> *lines = tw + L;
+     load_table<T>(tw, twline, L);
+     const int tid = threadIdx.x;
+     const int b = blockIdx.y;
+     const int k1b = blockIdx.x * LINES;
+#pragma unroll
+     for (int a = 0; a < NA; a++) {
+          const cx<T> *row0 = src.row(a, b, k1b);
+#pragma unroll 4
+          for (int idx = tid; idx < LINES * L; idx += L) {
+               int row = idx / L, n2 = idx % L;
+               lines[(a * LINES + row) * G::STRIDE + pad8(n2)] = row0[(size_t)row * src.rowstride + n2];
+          }
+     }
+     __syncthreads();
+     const int c = tid % LINES, t = tid / LINES;
+     cx<T> v[NA][8];
+     cx<T> *s[NA];
+#pragma unroll
+     for (int a = 0; a < NA; a++) {
+          s[a] = lines + (a * LINES + c) * G::STRIDE;
+#pragma unroll
+          for (int m = 0; m < 8; m++) v[a][m] = s[a][pad8(t + m * (L / 8))];
+     }
+     __syncthreads();
+     line_fft<T, L, SIGN, NA>(v, s, tw, t);
+     epi.template store<L>(v, b, k1b + c, t);
+}
+
+// ------------------------------------------------------------------ policies
+
+// Column-pass epilogue: multiply by W_N^(n2*k1) and store Y[k1*N2 + n2].
+// Batch b, array a lives at y + ((size_t)b*NA + a)*N.
+template <typename T, int SIGN, int NA>
+struct StoreFourstep {
+     cx<T> *y;
+     const cx<T> *hi, *lo;
+     int N2;
+     int N;
+     template <int L>
+     __device__ __forceinline__ void store(const cx<T> (&v)[NA][8], int b, int n2, int t) const {
+#pragma unroll
+          for (int a = 0; a < NA; a++) {
+               cx<T> *dst = y + ((size_t)b * NA + a) * N + n2;
+#pragma unroll
+               for (int m = 0; m < 8; m++) {
+                    int k1 = t + m * (L / 8);
+                    cx<T> w = twsign<SIGN>(fourstep_twiddle<T>(hi, lo, n2 * k1));
+                    dst[(size_t)k1 * N2] = cmul(v[a][m], w);
+               }
+          }
+     }
+};
+
+// Row-pass source: rows of Y laid out as in StoreFourstep.
+template <typename T, int NA>
+struct RowsY {
+     const cx<T> *y;
+     int N;          // N1*N2
+     int rowstride;  // N2
+     __device__ __forceinline__ const cx<T> *row(int a, int b, int k1) const {
+          return y + ((size_t)b * NA + a) * N + (size_t)k1 * rowstride;
+     }
+};
+
+// Row-pass epilogue: natural-order output X[k1 + N1*k2] * scale for k < nkeep.
+template <typename T>
+struct StoreNatural {
+     cx<T> *x;
+     int N1;
+     int N;          // array stride
+     int nkeep;
+     T scale;
+     template <int L>
+     __device__ __forceinline__ void store(const cx<T> (&v)[1][8], int b, int k1, int t) const {
+          cx<T> *dst = x + (size_t)b * N;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               int k = k1 + N1 * (t + m * (L / 8));
+               if (k < nkeep) dst[k] = cscale(v[0][m], scale);
+          }
+     }
+};
+
+// Column-pass prologue: plain load of x[N2*n1 + n2] from natural-order arrays
+// of stride N (arrays already zero-padded to N).
+template <typename T>
+struct LoadNatural {
+     const cx<T> *x;
+     int N2;
+     int N;
+     template <int L>
+     __device__ __forceinline__ void load(cx<T> (&v)[1][8], int b, int n2, int t) const {
+          const cx<T> *src = x + (size_t)b * N + n2;
+#pragma unroll
+          for (int m = 0; m < 8; m++) v[0][m] = src[(size_t)N2 * (t + m * (L / 8))];
+     }
+};
+
+// Column-pass prologue of the interpolation inverse FFT: the spectrum of
+// length nfft is spread to Ninterp = ratio*nfft, moving bins [nyqst, nfft)
+// to the top and zeroing the middle (jobcore.c:336-350).
+template <typename T>
+struct LoadShuffled {
+     const cx<T> *x;  // forward spectra (nfft values each), arrays `stride` apart
+     int N2;          // of the Ninterp transform
+     int stride;
+     int nfft;
+     int Ninterp;
+     template <int L>
+     __device__ __forceinline__ void load(cx<T> (&v)[1][8], int b, int n2, int t) const {
+          const cx<T> *src = x + (size_t)b * stride;
+          const int nyqst = nfft / 2 + 1;
+          const int gap = Ninterp - nfft;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               int k = N2 * (t + m * (L / 8)) + n2;
+               cx<T> z;
+               z.x = 0;
+               z.y = 0;
+               if (k < nyqst) z = src[k];
+               else if (k >= nyqst + gap) z = src[k - gap];
+               v[0][m] = z;
+          }
+     }
+};
+
+}  // namespace tdf

@@ -28,6 +28,18 @@ AU_LIGHT_S = 499.00478383615643      # 1 astronomical unit in light-seconds
 R_EARTH_LIGHT_S = 6378.140 / 299792.458
 
 
+def _cos(x: np.ndarray) -> np.ndarray:
+    """Element-wise cos through the C library (math.cos), so that generated
+    inputs do not depend on which SIMD path numpy picks on a given CPU."""
+    return np.fromiter((math.cos(v) for v in np.asarray(x, dtype=np.float64).ravel()), dtype=np.float64,
+                       count=np.size(x)).reshape(np.shape(x))
+
+
+def _sin(x: np.ndarray) -> np.ndarray:
+    return np.fromiter((math.sin(v) for v in np.asarray(x, dtype=np.float64).ravel()), dtype=np.float64,
+                       count=np.size(x)).reshape(np.shape(x))
+
+
 @dataclass
 class Injection:
     """A CW signal in add_signal()'s model (init.c:365-504), 'amp' form."""
@@ -107,12 +119,12 @@ def detssb(N: int, dt: float, name: str, phir: float, orbit_phase: float) -> np.
     om_y = 2.0 * math.pi / host.C_YEARSEC
     th = orbit_phase + om_y * t
     eps = host.C_EPSMA
-    ex = AU_LIGHT_S * np.cos(th)
-    ey = AU_LIGHT_S * np.sin(th) * math.cos(eps)
-    ez = AU_LIGHT_S * np.sin(th) * math.sin(eps)
+    ex = AU_LIGHT_S * _cos(th)
+    ey = AU_LIGHT_S * _sin(th) * math.cos(eps)
+    ez = AU_LIGHT_S * _sin(th) * math.sin(eps)
     ro = phir + host.C_OMEGA_R * t
-    rx = R_EARTH_LIGHT_S * math.cos(ephi) * np.cos(ro)
-    ry = R_EARTH_LIGHT_S * math.cos(ephi) * np.sin(ro)
+    rx = R_EARTH_LIGHT_S * math.cos(ephi) * _cos(ro)
+    ry = R_EARTH_LIGHT_S * math.cos(ephi) * _sin(ro)
     rz = R_EARTH_LIGHT_S * math.sin(ephi) * np.ones_like(t)
     out = np.empty(3 * N)
     out[0::3] = (ex + rx) / dt
@@ -177,7 +189,8 @@ def inject(case: Case, sett: host.Settings, dets: List[host.Detector], xdats: Li
         sh = ca * cd * e[0::3] + sa * cd * e[1::3] + sd * e[2::3]
         ph = freqo0 * (i + sh) + freqo1 * (2. * sh * i + i * i + sh * sh) + phaseshift
         ph -= 2 * math.pi * sett.dt * sett.fpo * i
-        s = amp[0] * aa * np.cos(ph) + amp[1] * bb * np.cos(ph) + amp[2] * aa * np.sin(ph) + amp[3] * bb * np.sin(ph)
+        cph, sph = _cos(ph), _sin(ph)
+        s = amp[0] * aa * cph + amp[1] * bb * cph + amp[2] * aa * sph + amp[3] * bb * sph
         sigs.append(s)
     h0 = inj.h0
     if inj.snr is not None:

@@ -1,0 +1,65 @@
+"""Generates the golden fixtures: runs the reference's own search (compiled
+from its unmodified sources by oracle/Makefile, FP64 and FP32 builds) on every
+case of cases.py and stores its trigger records.
+
+    python tests/golden/make_golden.py          (needs the reference tree; CPU only)
+
+Each fixture <name>.npz holds: input checksum, the reference's records
+(pm, m, n, s, ra, dec, fdot; lens; flat (f, F) pairs) for the f64 and f32
+builds, and their walltimes.
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, os.path.dirname(HERE))
+
+from tdfstat_b200 import synth  # noqa: E402
+import refkit  # noqa: E402
+from golden.cases import CASES, input_checksum  # noqa: E402
+
+
+def pack(recs):
+    lens = np.array([len(p) for p in recs.pairs], dtype=np.int64)
+    flat = np.concatenate(recs.pairs).astype(np.float32) if len(recs.pairs) and lens.sum() else np.zeros(0, np.float32)
+    return recs.hdr.astype(np.float32), lens, flat, recs.pm.astype(np.int32)
+
+
+def main(names=None):
+    refkit.build_oracle(ref=True)
+    for name, case in CASES.items():
+        if names and name not in names:
+            continue
+        root = tempfile.mkdtemp(prefix="tdfgold_")
+        try:
+            ini = synth.write_case(root, case)
+            cks = input_checksum(root)
+            out = {"checksum": np.array(cks)}
+            for which in ("f64", "f32"):
+                shutil.rmtree(os.path.join(root, "out"), ignore_errors=True)
+                # write_case put the veto-line file in out/; regenerate it
+                synth.write_case(root, case)
+                recs, meta, _ = refkit.run_reference(ini, which, threads=1)
+                hdr, lens, flat, pm = pack(recs)
+                out[which + "_hdr"] = hdr
+                out[which + "_lens"] = lens
+                out[which + "_pairs"] = flat
+                out[which + "_pm"] = pm
+                out[which + "_walltime"] = np.array(meta.get("walltime", 0.0))
+                print("%-20s %s: %d records, %d triggers, %.2fs" % (name, which, len(recs), recs.ntrig,
+                                                                    meta.get("walltime", 0.0)))
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        finally:
+            shutil.rmtree(root, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -206,6 +206,10 @@ def run_tdf(args, rank, world, local_rank):
     root = tempfile.mkdtemp(prefix="tdfbench_")
     try:
         wl = Workload(args.workload, root)
+        if args.sky_points:
+            wl.pm, wl.mm, wl.nn = wl.pm[:args.sky_points], wl.mm[:args.sky_points], wl.nn[:args.sky_points]
+            wl.config["sky_points"] = len(wl.pm)
+            wl.config["templates_per_step"] = len(wl.pm) * wl.nspd
         job = wl.job
         pm, mm, nn = wl.shard(rank, world)
         seg, opts = job.segment(), job.search_opts()
@@ -224,7 +228,6 @@ def run_tdf(args, rank, world, local_rank):
             eng.search_device(pm, mm, nn)
         torch.cuda.synchronize()
         # ---- value: device-resident inputs, K steps
-        eng.enable_kernel_timing(True)
         launches0 = eng.launch_count()
         clocks = ClockSampler(local_rank)
         clocks.start()
@@ -244,6 +247,14 @@ def run_tdf(args, rank, world, local_rank):
         clk = clocks.stop()
         ms = ev0.elapsed_time(ev1)
         launches = eng.launch_count() - launches0
+        # ---- per-kernel durations: the same K steps again with CUDA events
+        # recorded on the engine's stream around every launch
+        eng.enable_kernel_timing(True)
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            eng.search_device(pm, mm, nn)
+        torch.cuda.synchronize()
         ktimes = eng.kernel_times()
         eng.enable_kernel_timing(False)
         # ---- e2e: host buffers through the C ABI
@@ -367,6 +378,7 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
     ap.add_argument("--sky-batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sky-points", type=int, default=0, help="use only the first K sky points (profiling runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

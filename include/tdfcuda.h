@@ -140,6 +140,18 @@ int tdf_search_points(tdf_engine *e, int npts, const int32_t *pm, const float *m
                       float *pairs, int64_t max_pairs, int64_t *npairs,
                       int32_t *nrec_per_point);
 
+/* Number of records tdf_search_points() would produce for these points (host
+   arithmetic only, no device work): one per spindown of each point inside
+   the sky ellipse (jobcore.c:248,427).  nrec_per_point may be NULL. */
+int tdf_count_templates(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
+                        const float *sst, int64_t *nrec, int32_t *nrec_per_point);
+
+/* After tdf_search_points() returned TDF_ERR_CAPACITY the engine keeps the
+   results; this copies them into larger arrays without running the search
+   again.  Returns TDF_ERR_INVALID if no results are kept. */
+int tdf_last_results(tdf_engine *e, tdf_record *recs, int64_t max_recs, int64_t *nrec,
+                     float *pairs, int64_t max_pairs, int64_t *npairs, int32_t *nrec_per_point);
+
 /* Device-only pass: same work as tdf_search_points() but the trigger list
    stays on the device; returns the record and trigger counts.  Used to time
    the kernels with inputs resident in HBM. */

@@ -1,8 +1,7 @@
 """ctypes mirror of include/tdfcuda.h (the C ABI of libtdfcuda).
 
-The structure layouts here must match the header field for field; the
-library checks ``sizeof`` of each at load time through
-``tdf_abi_struct_sizes``.
+The structure layouts here must match the header field for field;
+tests/test_abi.py compares their sizes with what a C compiler gives.
 """
 import ctypes as C
 import os
@@ -119,6 +118,8 @@ ABI_FUNCTIONS = [
     ("tdf_engine_destroy", C.c_int, [P]),
     ("tdf_search_points", C.c_int,
      [P, C.c_int, I32P, F32P, F32P, F32P, RECP, C.c_int64, I64P, F32P, C.c_int64, I64P, I32P]),
+    ("tdf_count_templates", C.c_int, [P, C.c_int, I32P, F32P, F32P, F32P, I64P, I32P]),
+    ("tdf_last_results", C.c_int, [P, RECP, C.c_int64, I64P, F32P, C.c_int64, I64P, I32P]),
     ("tdf_search_points_device", C.c_int,
      [P, C.c_int, I32P, F32P, F32P, F32P, I64P, I64P]),
     ("tdf_fstat_spectrum", C.c_int,

@@ -61,6 +61,9 @@ static int ilog2i(int n) { int l = 0; while ((1 << l) < n) l++; return l; }
 template <class K>
 static int set_smem(K kern, size_t smem) {
      if (smem > 48 * 1024) CUCHK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+     // the FFT passes live in shared memory: ask for the largest carveout so
+     // that more than one CTA fits per SM
+     CUCHK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
      return TDF_OK;
 }
 
@@ -185,6 +188,9 @@ struct FFTTables {
      const cx<T> *o() const { return lo.as<cx<T>>(); }
 };
 
+// chunks whose F spectra share one trigger-selection launch
+constexpr int kGroup = 4;
+
 // host view of one template
 struct HostTmpl {
      int pt;         // index of the point in the call
@@ -212,7 +218,7 @@ struct tdf_engine {
      int N = 0, nfft = 0, nfftf = 0, Ninterp = 0, nifo = 0, Nal = 0, n2N = 0;
      int nF = 0, nblk_mu = 0;
      int Bs = 8;        // sky points per batch
-     int Tc = 32;       // templates per chunk
+     int Tc = 16;       // templates per chunk (intermediate spectra sized for L2)
      int64_t launches = 0;
      FFTTables<double> t_nfft, t_ninterp, t_f64;
      FFTTables<float> t_f32;
@@ -223,37 +229,51 @@ struct tdf_engine {
      // operands
      DevBuf xab, s2, xa64, xb64, t1;
      // spindown stage
-     DevBuf tparam, Ybuf, Fbuf, mubuf, trig, counters, tcnt, linesd;
+     DevBuf tparam, Ybuf, Fbuf, mubuf, tcnt, linesd, cand;
+     unsigned cand_cap = 0;
+     // two batch slots: while the host drains one slot's triggers the
+     // device runs the other slot's batch
+     DevBuf trig[2], counters[2];
      unsigned long long trig_cap = 0;
-     // pinned staging
-     SkyParam *h_sky = nullptr;
-     TmplParam *h_tp = nullptr;
+     SkyParam *h_sky[2] = {nullptr, nullptr};     // pinned staging per slot
+     TmplParam *h_tp[2] = {nullptr, nullptr};
      size_t h_tp_cap = 0;
-     unsigned long long *h_cnt = nullptr;
+     unsigned long long *h_cnt = nullptr;         // pinned [slot][count, error flags]
+     cudaEvent_t done[2] = {nullptr, nullptr};
+     int cur = 0;                                 // slot the kernels write to
      std::vector<Trig> h_trig;
+     // results of the last search kept after a TDF_ERR_CAPACITY return
+     bool kept = false;
+     std::vector<tdf_record> last_recs;
+     std::vector<float> last_pairs;
+     std::vector<int32_t> last_per;
      // optional per-kernel event timing
      bool timing = false;
      tdf_kernel_times kt{};
      std::vector<cudaEvent_t> evpool;
-     size_t evused = 0;
+     std::vector<size_t> evfree;
      struct Pending { int kind; size_t ev; int64_t templates; };
      std::vector<Pending> pending;
 };
 
 enum { KT_COL = 0, KT_ROW = 1, KT_THR = 2, KT_SKY = 3 };
 
-// records the opening event of a timed region; returns its pool index
+// records the opening event of a timed region; returns the index of an
+// event pair in the pool (pairs are recycled once collected)
 static size_t timing_begin(tdf_engine *e) {
-     if (e->evused + 2 > e->evpool.size()) {
-          for (int k = 0; k < 64; k++) {
-               cudaEvent_t ev;
-               if (cudaEventCreate(&ev) != cudaSuccess) break;
-               e->evpool.push_back(ev);
+     if (e->evfree.empty()) {
+          cudaEvent_t a, b;
+          if (cudaEventCreate(&a) != cudaSuccess) return (size_t)-1;
+          if (cudaEventCreate(&b) != cudaSuccess) {
+               cudaEventDestroy(a);
+               return (size_t)-1;
           }
+          e->evpool.push_back(a);
+          e->evpool.push_back(b);
+          e->evfree.push_back(e->evpool.size() - 2);
      }
-     size_t i = e->evused;
-     if (i + 2 > e->evpool.size()) return (size_t)-1;
-     e->evused += 2;
+     size_t i = e->evfree.back();
+     e->evfree.pop_back();
      cudaEventRecord(e->evpool[i], e->stream);
      return i;
 }
@@ -264,20 +284,25 @@ static void timing_end(tdf_engine *e, size_t i, int kind, int64_t templates) {
      e->pending.push_back({kind, i, templates});
 }
 
-// after a stream synchronisation: fold the recorded pairs into kt
+// folds the completed pairs (in recording order) into kt
 static void timing_collect(tdf_engine *e) {
-     for (const auto &p : e->pending) {
+     size_t k = 0;
+     for (; k < e->pending.size(); k++) {
+          const auto &p = e->pending[k];
+          if (cudaEventQuery(e->evpool[p.ev + 1]) != cudaSuccess) break;
           float ms = 0.f;
-          if (cudaEventElapsedTime(&ms, e->evpool[p.ev], e->evpool[p.ev + 1]) != cudaSuccess) continue;
-          switch (p.kind) {
-          case KT_COL: e->kt.colpass_ms += ms; e->kt.colpass_launches++; e->kt.colpass_templates += p.templates; break;
-          case KT_ROW: e->kt.rowpass_ms += ms; e->kt.rowpass_launches++; break;
-          case KT_THR: e->kt.threshold_ms += ms; e->kt.threshold_launches++; break;
-          case KT_SKY: e->kt.sky_ms += ms; e->kt.sky_batches++; break;
+          if (cudaEventElapsedTime(&ms, e->evpool[p.ev], e->evpool[p.ev + 1]) == cudaSuccess) {
+               switch (p.kind) {
+               case KT_COL: e->kt.colpass_ms += ms; e->kt.colpass_launches++; e->kt.colpass_templates += p.templates; break;
+               case KT_ROW: e->kt.rowpass_ms += ms; e->kt.rowpass_launches++; break;
+               case KT_THR: e->kt.threshold_ms += ms; e->kt.threshold_launches++; break;
+               case KT_SKY: e->kt.sky_ms += ms; e->kt.sky_batches++; break;
+               }
           }
+          e->evfree.push_back(p.ev);
      }
-     e->pending.clear();
-     e->evused = 0;
+     cudaGetLastError();   // a not-ready query leaves no sticky error, clear it anyway
+     e->pending.erase(e->pending.begin(), e->pending.begin() + k);
 }
 
 static size_t Wstride(const tdf_engine *e) { return (size_t)e->Ninterp; }
@@ -371,17 +396,24 @@ static int engine_alloc(tdf_engine *e) {
      const size_t csz = e->form == TDF_FORM_SPLIT ? sizeof(float2) : sizeof(double2);
      const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
      TRY(e->Ybuf.alloc((size_t)Tc * 2 * e->nfftf * csz));
-     TRY(e->Fbuf.alloc((size_t)Tc * e->nF * rsz));
-     TRY(e->mubuf.alloc((size_t)Tc * std::max(1, e->nblk_mu) * rsz));
-     TRY(e->tcnt.alloc(Tc * sizeof(unsigned)));
-     TRY(e->counters.alloc(2 * sizeof(unsigned long long)));
+     const size_t G = (size_t)kGroup * Tc;   // templates per resolve group
+     TRY(e->Fbuf.alloc(G * e->nF * rsz));
+     TRY(e->mubuf.alloc(G * std::max(1, e->nblk_mu) * rsz));
+     TRY(e->tcnt.alloc((G + 1) * sizeof(unsigned)));
+     e->cand_cap = (unsigned)G * 4096u;
+     TRY(e->cand.alloc(e->cand_cap * sizeof(uint2)));
      TRY(e->linesd.alloc(std::max<size_t>(1, e->lines.size()) * sizeof(double)));
      if (!e->lines.empty())
           CUCHK(cudaMemcpy(e->linesd.p, e->lines.data(), e->lines.size() * sizeof(double), cudaMemcpyHostToDevice));
-     e->trig_cap = 1ull << 22;
-     TRY(e->trig.alloc(e->trig_cap * sizeof(Trig)));
-     CUCHK(cudaMallocHost((void **)&e->h_sky, Bs * sizeof(SkyParam)));
-     CUCHK(cudaMallocHost((void **)&e->h_cnt, 2 * sizeof(unsigned long long)));
+     e->trig_cap = 1ull << 21;
+     for (int s = 0; s < 2; s++) {
+          TRY(e->counters[s].alloc(2 * sizeof(unsigned long long)));
+          CUCHK(cudaMemset(e->counters[s].p, 0, 2 * sizeof(unsigned long long)));
+          TRY(e->trig[s].alloc(e->trig_cap * sizeof(Trig)));
+          CUCHK(cudaMallocHost((void **)&e->h_sky[s], Bs * sizeof(SkyParam)));
+          CUCHK(cudaEventCreateWithFlags(&e->done[s], cudaEventDisableTiming));
+     }
+     CUCHK(cudaMallocHost((void **)&e->h_cnt, 4 * sizeof(unsigned long long)));
      TRY(e->t_nfft.build(e->nfft));
      TRY(e->t_ninterp.build(e->Ninterp));
      if (e->form == TDF_FORM_SPLIT) TRY(e->t_f32.build(e->nfftf));
@@ -392,21 +424,27 @@ static int engine_alloc(tdf_engine *e) {
 static void engine_free(tdf_engine *e) {
      DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp,
                        &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb, &e->xab, &e->s2,
-                       &e->xa64, &e->xb64, &e->t1, &e->tparam, &e->Ybuf, &e->Fbuf, &e->mubuf, &e->trig,
-                       &e->counters, &e->tcnt, &e->linesd};
+                       &e->xa64, &e->xb64, &e->t1, &e->tparam, &e->Ybuf, &e->Fbuf, &e->mubuf,
+                       &e->trig[0], &e->trig[1], &e->counters[0], &e->counters[1], &e->tcnt, &e->linesd, &e->cand};
      for (DevBuf *b : bufs) b->release();
      e->t_nfft.release();
      e->t_ninterp.release();
      e->t_f32.release();
      e->t_f64.release();
-     if (e->h_sky) cudaFreeHost(e->h_sky);
-     if (e->h_tp) cudaFreeHost(e->h_tp);
+     for (int s = 0; s < 2; s++) {
+          if (e->h_sky[s]) cudaFreeHost(e->h_sky[s]);
+          if (e->h_tp[s]) cudaFreeHost(e->h_tp[s]);
+          if (e->done[s]) cudaEventDestroy(e->done[s]);
+          e->h_sky[s] = nullptr;
+          e->h_tp[s] = nullptr;
+          e->done[s] = nullptr;
+     }
      if (e->h_cnt) cudaFreeHost(e->h_cnt);
-     e->h_sky = nullptr;
-     e->h_tp = nullptr;
      e->h_cnt = nullptr;
      for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
      e->evpool.clear();
+     e->evfree.clear();
+     e->pending.clear();
      if (e->own) cudaStreamDestroy(e->own);
      e->own = nullptr;
 }
@@ -486,7 +524,7 @@ static int run_sky_stage(tdf_engine *e, int npts) {
      cudaStream_t st = e->stream;
      const int nifo = e->nifo, Q = npts * nifo;
      const size_t ws = Wstride(e);
-     CUCHK(cudaMemcpyAsync(e->skyp.p, e->h_sky, npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
+     CUCHK(cudaMemcpyAsync(e->skyp.p, e->h_sky[e->cur], npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
      const int nblk = e->nfft / 256;
      const bool split = e->form == TDF_FORM_SPLIT;
      k_sky_prep<<<dim3(nblk, Q), 256, 0, st>>>(
@@ -541,70 +579,142 @@ static int run_sky_stage(tdf_engine *e, int npts) {
      return TDF_OK;
 }
 
-// spindown stage for templates [t0, t0+nt) of the staged parameter array
+// Spindown stage, FFT part, for chunk `ci` of a resolve group whose templates
+// start at dtp: the column pass (demodulation + first FFT pass) and the row
+// pass (second FFT pass + F + candidate bins) for nt templates.
 template <typename T>
-static int run_chunk(tdf_engine *e, const TmplParam *dtp, int nt) {
+static int run_chunk(tdf_engine *e, const TmplParam *dtp, int ci, int nt) {
      cudaStream_t st = e->stream;
-     const bool split = std::is_same<T, float>::value;
      const FFTTables<T> *tb;
      if constexpr (std::is_same<T, float>::value) tb = &e->t_f32;
      else tb = &e->t_f64;
      const FFTTables<T> &t = *tb;
-     CUCHK(cudaMemsetAsync(e->tcnt.p, 0, nt * sizeof(unsigned), st));
+     const int boff = ci * e->Tc;
+     const TmplParam *ctp = dtp + boff;
+     const unsigned G = (unsigned)kGroup * e->Tc;
+     unsigned *tcnt = e->tcnt.as<unsigned>();
      StoreFourstep<T, -1, 2> epi{e->Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
      size_t tev = e->timing ? timing_begin(e) : (size_t)-1;
      if constexpr (std::is_same<T, float>::value) {
-          DemodSplit pro{e->xab.as<float4>(), e->s2.as<float>(), dtp, e->N, t.N2, e->Nal, e->nifo};
+          DemodSplit pro{e->xab.as<float4>(), e->s2.as<float>(), ctp, e->N, t.N2, e->Nal, e->nifo};
           TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
      } else {
-          DemodFP64 pro{e->xa64.as<double2>(), e->xb64.as<double2>(), e->t1.as<double>(), dtp, e->N, t.N2, e->Nal, e->nifo};
+          DemodFP64 pro{e->xa64.as<double2>(), e->xb64.as<double2>(), e->t1.as<double>(), ctp, e->N, t.N2, e->Nal, e->nifo};
           TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
      }
      if (e->timing) timing_end(e, tev, KT_COL, nt);
+     const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
      RowsY<T, 2> src{e->Ybuf.as<cx<T>>(), e->nfftf, t.N2};
-     StoreFstat<T> epi2{e->Fbuf.as<T>(), dtp, e->aabb.as<AaBb>(), e->nF, e->opts.fr[0], e->opts.fr[1], t.N1};
+     StoreFstat<T> epi2{e->Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb.as<AaBb>(), e->nF, e->opts.fr[0],
+                        e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : e->cand.as<uint2>(), tcnt + G,
+                        e->cand_cap, boff};
      tev = e->timing ? timing_begin(e) : (size_t)-1;
      TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
      if (e->timing) timing_end(e, tev, KT_ROW, nt);
      e->launches += 2;
-     const T *mu = nullptr;
-     if (e->opts.blocks_avg && e->nblk_mu > 0) {
-          k_block_means<T><<<dim3(e->nblk_mu, nt), 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->nblk_mu, e->mubuf.as<T>());
+     return TDF_OK;
+}
+
+// Trigger selection for the ntg templates of a resolve group (starting at
+// dtp; their F spectra fill the F ring in order): the candidate bins the row
+// passes collected, or, with blocks_avg, block means and a scan of every bin.
+template <typename T>
+static int run_resolve(tdf_engine *e, const TmplParam *dtp, int ntg) {
+     cudaStream_t st = e->stream;
+     const bool split = std::is_same<T, float>::value;
+     const unsigned G = (unsigned)kGroup * e->Tc;
+     unsigned *tcnt = e->tcnt.as<unsigned>();
+     const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
+     unsigned long long *cnt = e->counters[e->cur].as<unsigned long long>();
+     ThrArgs A;
+     A.nF = e->nF;
+     A.fr0 = e->opts.fr[0];
+     A.fr1 = e->opts.fr[1];
+     A.thr = e->opts.thr;
+     A.nblk = blocks ? e->nblk_mu : 0;
+     A.tp = dtp;
+     A.nfftf = e->nfftf;
+     A.lines = e->linesd.as<double>();
+     A.numlines = e->opts.numlines;
+     A.bufhalf = (unsigned)(e->opts.bufsize / 2);
+     A.trig = e->trig[e->cur].as<Trig>();
+     A.cap = e->trig_cap;
+     A.cnt = cnt;
+     A.tcnt = tcnt;
+     A.err = reinterpret_cast<unsigned *>(cnt + 1);
+     size_t tev = e->timing ? timing_begin(e) : (size_t)-1;
+     if (blocks) {
+          k_block_means<T><<<dim3(e->nblk_mu, ntg), 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->nblk_mu, e->mubuf.as<T>());
           CUCHK(cudaGetLastError());
-          mu = e->mubuf.as<T>();
+          dim3 g((e->nF + 255) / 256, ntg);
+          if (split) k_threshold<T, false><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->mubuf.as<T>(), A);
+          else k_threshold<T, true><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->mubuf.as<T>(), A);
+          e->launches += 2;
+     } else {
+          if (split) k_resolve<T, false><<<64, 256, 0, st>>>(e->Fbuf.as<T>(), A, e->cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
+          else k_resolve<T, true><<<64, 256, 0, st>>>(e->Fbuf.as<T>(), A, e->cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
           e->launches++;
      }
-     unsigned long long *cnt = e->counters.as<unsigned long long>();
-     dim3 g((e->nF + 255) / 256, nt);
-     tev = e->timing ? timing_begin(e) : (size_t)-1;
-     if (split)
-          k_threshold<T, false><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->opts.fr[0], e->opts.fr[1], e->opts.thr, mu,
-                                                    e->nblk_mu, dtp, e->nfftf, e->linesd.as<double>(), e->opts.numlines,
-                                                    (unsigned)(e->opts.bufsize / 2), e->trig.as<Trig>(), e->trig_cap, cnt,
-                                                    e->tcnt.as<unsigned>(), reinterpret_cast<unsigned *>(cnt + 1));
-     else
-          k_threshold<T, true><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->opts.fr[0], e->opts.fr[1], e->opts.thr, mu,
-                                                   e->nblk_mu, dtp, e->nfftf, e->linesd.as<double>(), e->opts.numlines,
-                                                   (unsigned)(e->opts.bufsize / 2), e->trig.as<Trig>(), e->trig_cap, cnt,
-                                                   e->tcnt.as<unsigned>(), reinterpret_cast<unsigned *>(cnt + 1));
      CUCHK(cudaGetLastError());
-     if (e->timing) timing_end(e, tev, KT_THR, nt);
-     e->launches++;
+     if (e->timing) timing_end(e, tev, KT_THR, ntg);
+     // ready for the next group: trigger counters and candidate count
+     CUCHK(cudaMemsetAsync(tcnt, 0, (G + 1) * sizeof(unsigned), st));
+     return TDF_OK;
+}
+
+// the spindown stage of nt templates starting at dtp: groups of chunks
+static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
+     const int G = kGroup * e->Tc;
+     for (int g0 = 0; g0 < nt; g0 += G) {
+          const int ntg = std::min(G, nt - g0);
+          for (int ci = 0; ci * e->Tc < ntg; ci++) {
+               const int n = std::min(e->Tc, ntg - ci * e->Tc);
+               if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, dtp + g0, ci, n));
+               else TRY(run_chunk<double>(e, dtp + g0, ci, n));
+          }
+          if (e->form == TDF_FORM_SPLIT) TRY(run_resolve<float>(e, dtp + g0, ntg));
+          else TRY(run_resolve<double>(e, dtp + g0, ntg));
+     }
      return TDF_OK;
 }
 
 static int ensure_tparam(tdf_engine *e, size_t n) {
      if (n > e->h_tp_cap) {
-          if (e->h_tp) {
-               CUCHK(cudaStreamSynchronize(e->stream));
-               cudaFreeHost(e->h_tp);
-               e->h_tp = nullptr;
-          }
+          CUCHK(cudaStreamSynchronize(e->stream));
           size_t cap = std::max<size_t>(n, 4096);
-          CUCHK(cudaMallocHost((void **)&e->h_tp, cap * sizeof(TmplParam)));
+          for (int s = 0; s < 2; s++) {
+               if (e->h_tp[s]) cudaFreeHost(e->h_tp[s]);
+               e->h_tp[s] = nullptr;
+               CUCHK(cudaMallocHost((void **)&e->h_tp[s], cap * sizeof(TmplParam)));
+          }
           e->h_tp_cap = cap;
           TRY(e->tparam.alloc(cap * sizeof(TmplParam)));
      }
+     return TDF_OK;
+}
+
+// Waits for the batch last run in `slot`, checks its flags and collects its
+// triggers; *over is set when the trigger buffer was too small.
+static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_total, bool *over) {
+     CUCHK(cudaEventSynchronize(e->done[slot]));
+     if (e->timing) timing_collect(e);
+     const unsigned long long nfound = e->h_cnt[2 * slot];
+     const unsigned errf = (unsigned)(e->h_cnt[2 * slot + 1] & 0xffffffffu);
+     if (errf & ERR_OVERFLOW)
+          return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
+     if (nfound > e->trig_cap) {
+          *over = true;
+          e->h_cnt[2 * slot] = nfound;   // keep the needed size visible
+          return TDF_OK;
+     }
+     *ntrig_total += (int64_t)nfound;
+     if (collect && nfound) {
+          size_t o = e->h_trig.size();
+          e->h_trig.resize(o + nfound);
+          // the batch is complete (event above); the engine stream may run on
+          CUCHK(cudaMemcpy(e->h_trig.data() + o, e->trig[slot].p, nfound * sizeof(Trig), cudaMemcpyDeviceToHost));
+     }
+     CUCHK(cudaMemsetAsync(e->counters[slot].p, 0, 2 * sizeof(unsigned long long), e->stream));
      return TDF_OK;
 }
 
@@ -631,79 +741,85 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
                tm.push_back(T);
           }
      }
-     e->h_trig.clear();
-     *ntrig_total = 0;
-     unsigned long long *cnt = e->counters.as<unsigned long long>();
-     CUCHK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), e->stream));
      // sky batches of consecutive inside points
      std::vector<int> inside;
      for (int i = 0; i < npts; i++)
           if (pts[i].inside && pts[i].iss_size > 0) inside.push_back(i);
+     size_t maxnt = 0;
      for (size_t b0 = 0; b0 < inside.size(); b0 += e->Bs) {
-          const int nb = (int)std::min<size_t>(e->Bs, inside.size() - b0);
-          CUCHK(cudaStreamSynchronize(e->stream));   // pinned staging reuse
-          int nt = 0;
-          for (int k = 0; k < nb; k++) {
-               const HostPoint &P = pts[inside[b0 + k]];
-               e->h_sky[k] = P.sp;
-               nt += P.iss_size;
-          }
-          TRY(ensure_tparam(e, nt));
-          int w = 0;
-          for (int k = 0; k < nb; k++) {
-               const HostPoint &P = pts[inside[b0 + k]];
-               for (int s = 0; s < P.iss_size; s++) {
-                    const HostTmpl &T = tm[P.first_tmpl + s];
-                    TmplParam &q = e->h_tp[w++];
-                    q.het1 = T.het1;
-                    q.spnd = T.spnd;
-                    q.sgnl0 = T.sgnl0;
-                    q.slot = k;
-                    q.id = (uint32_t)(P.first_tmpl + s);
-               }
-          }
-          size_t sev = e->timing ? timing_begin(e) : (size_t)-1;
-          TRY(run_sky_stage(e, nb));
-          if (e->timing) timing_end(e, sev, KT_SKY, nb);
-          CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp, nt * sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
-          for (int c0 = 0; c0 < nt; c0 += e->Tc) {
-               const int n = std::min(e->Tc, nt - c0);
-               if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, e->tparam.as<TmplParam>() + c0, n));
-               else TRY(run_chunk<double>(e, e->tparam.as<TmplParam>() + c0, n));
-          }
-          // drain this batch's triggers
-          CUCHK(cudaMemcpyAsync(e->h_cnt, cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
-          CUCHK(cudaStreamSynchronize(e->stream));
-          if (e->timing) timing_collect(e);
-          const unsigned long long nfound = e->h_cnt[0];
-          const unsigned errf = (unsigned)(e->h_cnt[1] & 0xffffffffu);
-          if (errf & ERR_OVERFLOW)
-               return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
-          if (nfound > e->trig_cap) {
-               // grow the trigger buffer and redo this batch's spindown stage
-               CUCHK(cudaStreamSynchronize(e->stream));
-               e->trig_cap = std::max<unsigned long long>(nfound + (nfound >> 2), e->trig_cap * 2);
-               e->trig.release();
-               TRY(e->trig.alloc(e->trig_cap * sizeof(Trig)));
-               CUCHK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), e->stream));
-               for (int c0 = 0; c0 < nt; c0 += e->Tc) {
-                    const int n = std::min(e->Tc, nt - c0);
-                    if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, e->tparam.as<TmplParam>() + c0, n));
-                    else TRY(run_chunk<double>(e, e->tparam.as<TmplParam>() + c0, n));
-               }
-               CUCHK(cudaMemcpyAsync(e->h_cnt, cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
-               CUCHK(cudaStreamSynchronize(e->stream));
-          }
-          const unsigned long long got = e->h_cnt[0];
-          *ntrig_total += (int64_t)got;
-          if (collect && got) {
-               size_t o = e->h_trig.size();
-               e->h_trig.resize(o + got);
-               CUCHK(cudaMemcpyAsync(e->h_trig.data() + o, e->trig.p, got * sizeof(Trig), cudaMemcpyDeviceToHost, e->stream));
-          }
-          CUCHK(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), e->stream));
+          size_t nt = 0;
+          for (size_t k = b0; k < std::min(inside.size(), b0 + e->Bs); k++) nt += pts[inside[k]].iss_size;
+          maxnt = std::max(maxnt, nt);
      }
-     CUCHK(cudaStreamSynchronize(e->stream));
+     TRY(ensure_tparam(e, maxnt));
+     for (int attempt = 0;; attempt++) {
+          e->h_trig.clear();
+          *ntrig_total = 0;
+          CUCHK(cudaStreamSynchronize(e->stream));
+          for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
+          CUCHK(cudaMemsetAsync(e->tcnt.p, 0, e->tcnt.bytes, e->stream));
+          int pending[2] = {0, 0};
+          bool over = false;
+          size_t b = 0;
+          for (size_t b0 = 0; b0 < inside.size(); b0 += e->Bs, b++) {
+               const int slot = (int)(b & 1);
+               // the slot's previous batch must be drained before its staging
+               // and trigger buffer are reused; the other slot keeps running
+               if (pending[slot]) {
+                    TRY(finish_slot(e, slot, collect, ntrig_total, &over));
+                    pending[slot] = 0;
+                    if (over) break;
+               }
+               e->cur = slot;
+               const int nb = (int)std::min<size_t>(e->Bs, inside.size() - b0);
+               int nt = 0;
+               for (int k = 0; k < nb; k++) {
+                    const HostPoint &P = pts[inside[b0 + k]];
+                    e->h_sky[slot][k] = P.sp;
+                    nt += P.iss_size;
+               }
+               int w = 0;
+               for (int k = 0; k < nb; k++) {
+                    const HostPoint &P = pts[inside[b0 + k]];
+                    for (int s = 0; s < P.iss_size; s++) {
+                         const HostTmpl &T = tm[P.first_tmpl + s];
+                         TmplParam &q = e->h_tp[slot][w++];
+                         q.het1 = T.het1;
+                         q.spnd = T.spnd;
+                         q.sgnl0 = T.sgnl0;
+                         q.slot = k;
+                         q.id = (uint32_t)(P.first_tmpl + s);
+                    }
+               }
+               size_t sev = e->timing ? timing_begin(e) : (size_t)-1;
+               TRY(run_sky_stage(e, nb));
+               if (e->timing) timing_end(e, sev, KT_SKY, nb);
+               CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[slot], nt * sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
+               TRY(run_templates(e, e->tparam.as<TmplParam>(), nt));
+               CUCHK(cudaMemcpyAsync(e->h_cnt + 2 * slot, e->counters[slot].p, 2 * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, e->stream));
+               CUCHK(cudaEventRecord(e->done[slot], e->stream));
+               pending[slot] = 1;
+          }
+          // drain in batch order: the slot of the second-to-last batch first
+          for (int k = 0; k < 2 && !over; k++) {
+               const int slot = (int)((b + k) & 1);
+               if (pending[slot]) {
+                    TRY(finish_slot(e, slot, collect, ntrig_total, &over));
+                    pending[slot] = 0;
+               }
+          }
+          CUCHK(cudaStreamSynchronize(e->stream));
+          if (!over) break;
+          if (attempt > 2) return set_error(TDF_ERR_CAPACITY, "trigger buffer could not be sized");
+          // a batch found more triggers than the buffer holds: grow and rerun
+          unsigned long long need = std::max(e->h_cnt[0], e->h_cnt[2]);
+          e->trig_cap = std::max<unsigned long long>(need + (need >> 2), e->trig_cap * 2);
+          for (int s = 0; s < 2; s++) {
+               e->trig[s].release();
+               TRY(e->trig[s].alloc(e->trig_cap * sizeof(Trig)));
+          }
+     }
      return TDF_OK;
 }
 
@@ -825,6 +941,7 @@ int tdf_search_points(tdf_engine *e, int npts, const int32_t *pm, const float *m
      std::vector<HostPoint> pts;
      std::vector<HostTmpl> tm;
      int64_t ntrig = 0;
+     e->kept = false;
      TRY(search_core(e, npts, pm, mm, nn, sst, pts, tm, true, &ntrig));
      // sort triggers into (template, bin) order: the reference's order
      std::vector<Trig> &tg = e->h_trig;
@@ -836,9 +953,16 @@ int tdf_search_points(tdf_engine *e, int npts, const int32_t *pm, const float *m
      *npairs = need_pairs;
      if (nrec_per_point)
           for (int i = 0; i < npts; i++) nrec_per_point[i] = pts[i].inside ? pts[i].iss_size : 0;
-     if (need_recs > max_recs || need_pairs > max_pairs || (need_recs && !recs) || (need_pairs && !pairs))
-          return set_error(TDF_ERR_CAPACITY, "need %lld records and %lld floats", (long long)need_recs,
-                           (long long)need_pairs);
+     const bool fits = !(need_recs > max_recs || need_pairs > max_pairs || (need_recs && !recs) || (need_pairs && !pairs));
+     if (!fits) {
+          // keep the results for tdf_last_results()
+          e->last_recs.resize(need_recs);
+          e->last_pairs.resize(need_pairs);
+          e->last_per.assign(npts, 0);
+          for (int i = 0; i < npts; i++) e->last_per[i] = pts[i].inside ? pts[i].iss_size : 0;
+          recs = e->last_recs.data();
+          pairs = e->last_pairs.data();
+     }
      size_t k = 0;
      int64_t off = 0;
      for (size_t t = 0; t < tm.size(); t++) {
@@ -862,6 +986,43 @@ int tdf_search_points(tdf_engine *e, int npts, const int32_t *pm, const float *m
           }
           r.len = len;
      }
+     if (!fits) {
+          e->kept = true;
+          return set_error(TDF_ERR_CAPACITY, "need %lld records and %lld floats", (long long)need_recs,
+                           (long long)need_pairs);
+     }
+     return TDF_OK;
+}
+
+int tdf_last_results(tdf_engine *e, tdf_record *recs, int64_t max_recs, int64_t *nrec, float *pairs,
+                     int64_t max_pairs, int64_t *npairs, int32_t *nrec_per_point) {
+     if (!e || !nrec || !npairs) return set_error(TDF_ERR_INVALID, "null engine or count pointers");
+     if (!e->kept) return set_error(TDF_ERR_INVALID, "no results kept from a previous tdf_search_points() call");
+     *nrec = (int64_t)e->last_recs.size();
+     *npairs = (int64_t)e->last_pairs.size();
+     if (*nrec > max_recs || *npairs > max_pairs || (*nrec && !recs) || (*npairs && !pairs))
+          return set_error(TDF_ERR_CAPACITY, "need %lld records and %lld floats", (long long)*nrec, (long long)*npairs);
+     if (*nrec) memcpy(recs, e->last_recs.data(), *nrec * sizeof(tdf_record));
+     if (*npairs) memcpy(pairs, e->last_pairs.data(), *npairs * sizeof(float));
+     if (nrec_per_point && !e->last_per.empty())
+          memcpy(nrec_per_point, e->last_per.data(), e->last_per.size() * sizeof(int32_t));
+     return TDF_OK;
+}
+
+int tdf_count_templates(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
+                        const float *sst, int64_t *nrec, int32_t *nrec_per_point) {
+     if (!e || !nrec) return set_error(TDF_ERR_INVALID, "null engine or count pointer");
+     if (npts < 0 || (npts > 0 && (!pm || !mm || !nn))) return set_error(TDF_ERR_INVALID, "bad sky point arrays");
+     int64_t n = 0;
+     for (int i = 0; i < npts; i++) {
+          if (pm[i] != 1 && pm[i] != 2) return set_error(TDF_ERR_INVALID, "pm[%d]=%d (must be 1 or 2)", i, pm[i]);
+          HostPoint P;
+          point_setup(e, pm[i], mm[i], nn[i], sst ? sst[i] : e->opts.spndr[0], P);
+          const int c = P.inside ? P.iss_size : 0;
+          if (nrec_per_point) nrec_per_point[i] = c;
+          n += c;
+     }
+     *nrec = n;
      return TDF_OK;
 }
 
@@ -887,19 +1048,20 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      HostTmpl T;
      tmpl_setup(e, P, mm, nn, ss, T);
      CUCHK(cudaStreamSynchronize(e->stream));
-     e->h_sky[0] = P.sp;
      TRY(ensure_tparam(e, 1));
-     TmplParam &q = e->h_tp[0];
+     e->cur = 0;
+     e->h_sky[0][0] = P.sp;
+     TmplParam &q = e->h_tp[0][0];
      q.het1 = T.het1;
      q.spnd = T.spnd;
      q.sgnl0 = T.sgnl0;
      q.slot = 0;
      q.id = 0;
      TRY(run_sky_stage(e, 1));
-     CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp, sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
-     CUCHK(cudaMemsetAsync(e->counters.p, 0, 2 * sizeof(unsigned long long), e->stream));
-     if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, e->tparam.as<TmplParam>(), 1));
-     else TRY(run_chunk<double>(e, e->tparam.as<TmplParam>(), 1));
+     CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[0], sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
+     CUCHK(cudaMemsetAsync(e->counters[0].p, 0, 2 * sizeof(unsigned long long), e->stream));
+     CUCHK(cudaMemsetAsync(e->tcnt.p, 0, e->tcnt.bytes, e->stream));
+     TRY(run_templates(e, e->tparam.as<TmplParam>(), 1));
      const int n = e->nF;
      if (e->form == TDF_FORM_SPLIT) {
           std::vector<float> f(n), mu(std::max(1, e->nblk_mu));

@@ -175,23 +175,24 @@ int tdf_job_core_ref(int pm, float mm, float nn, tdf_ref_Search_settings *sett, 
      int64_t nrec = 0, npairs = 0;
      struct timespec t0, t1;
      clock_gettime(CLOCK_MONOTONIC, &t0);
-     for (int attempt = 0; attempt < 2; attempt++) {
-          int st = tdf_search_points(S.eng, 1, &p, &m, &n, &s0, S.recs.data(), (int64_t)S.recs.size(), &nrec,
-                                     S.pairs.data(), (int64_t)S.pairs.size(), &npairs, nullptr);
-          if (st == TDF_ERR_CAPACITY && attempt == 0) {
-               S.recs.resize(nrec);
-               S.pairs.resize(npairs);
-               continue;
-          }
-          if (st == TDF_ERR_TRIGGER_OVERFLOW) {
-               printf("\n[ERROR] Too many triggers! buffer_size=%d [triggers]\n", sett->bufsize / 2);
-               printf("\nFAILURE\n");
-               fflush(stdout);
-               exit(EXIT_FAILURE);
-          }
-          if (st != TDF_OK) die("job_core", st);
-          break;
+     int st = tdf_count_templates(S.eng, 1, &p, &m, &n, &s0, &nrec, nullptr);
+     if (st != TDF_OK) die("job_core", st);
+     if ((int64_t)S.recs.size() < nrec) S.recs.resize(nrec);
+     st = tdf_search_points(S.eng, 1, &p, &m, &n, &s0, S.recs.data(), (int64_t)S.recs.size(), &nrec,
+                            S.pairs.data(), (int64_t)S.pairs.size(), &npairs, nullptr);
+     if (st == TDF_ERR_CAPACITY) {
+          // the engine kept the results; fetch them into larger arrays
+          S.recs.resize(nrec);
+          S.pairs.resize(npairs);
+          st = tdf_last_results(S.eng, S.recs.data(), nrec, &nrec, S.pairs.data(), npairs, &npairs, nullptr);
      }
+     if (st == TDF_ERR_TRIGGER_OVERFLOW) {
+          printf("\n[ERROR] Too many triggers! buffer_size=%d [triggers]\n", sett->bufsize / 2);
+          printf("\nFAILURE\n");
+          fflush(stdout);
+          exit(EXIT_FAILURE);
+     }
+     if (st != TDF_OK) die("job_core", st);
      clock_gettime(CLOCK_MONOTONIC, &t1);
      int ntrig = 0, maxt = 0;
      for (int64_t r = 0; r < nrec; r++) {

@@ -18,9 +18,12 @@
 // v[m] = x[t + m*L/8] on entry and v[m] = X[t + m*L/8] on exit (m < 8).
 //
 // Shared-memory layout: element p of a line sits at pad(p) = p + p/8 inside
-// the line, lines are LSTRIDE elements apart; LSTRIDE is chosen so that the
-// 32 lanes of a warp (8 lines x 4 consecutive t) spread evenly over the
-// banks for both float2 and double2 elements.
+// the line, lines are STRIDE elements apart.  Lane l of a warp works on line
+// l % 8 at position t = l / 8.  64-bit accesses are serviced per half-warp
+// (8 lines x 2 consecutive t) and 128-bit accesses per quarter-warp (8 lines,
+// one t), so STRIDE = 2 (mod 16) for float2 and odd for double2 puts the
+// lanes of each phase on distinct banks for every load/store pattern of the
+// Stockham passes.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -105,8 +108,8 @@ __device__ __forceinline__ int pad8(int p) { return p + (p >> 3); }
 
 template <typename T, int L> struct LineGeom {
      static constexpr int LP = L + L / 8;   // padded line length
-     // bank-spreading line stride: == 4 (mod 16) for 8-byte, == 2 (mod 8) for 16-byte elements
-     static constexpr int STRIDE = sizeof(cx<T>) == 8 ? LP + ((4 - LP % 16) + 16) % 16 : LP + ((2 - LP % 8) + 8) % 8;
+     // bank-spreading line stride: == 2 (mod 16) for 8-byte, odd for 16-byte elements
+     static constexpr int STRIDE = sizeof(cx<T>) == 8 ? LP + ((2 - LP % 16) + 16) % 16 : LP + (LP % 2 == 0 ? 1 : 0);
      static constexpr int NT = L / 8;       // threads per line
      static constexpr int P8 = ilog8(L);    // radix-8 passes
      static constexpr int RL = L / ipow8(ilog8(L));   // last radix (1 = none)
@@ -115,7 +118,8 @@ template <typename T, int L> struct LineGeom {
 constexpr int LINES = 8;   // lines (columns or rows) per CTA
 
 // Apply the Stockham twiddles of a pass (radix R, span NS) to the butterflies
-// a thread owns.  tw[m] = e^{-2 pi i m / L}, m < L (shared memory).
+// a thread owns.  tw[m] = e^{-2 pi i m / L}, m < L (shared memory).  Powers
+// 1, 2, 4 come from the table, the others as products of two of them.
 template <typename T, int L, int R, int SIGN>
 __device__ __forceinline__ void pass_twiddle(cx<T> (&v)[8], const cx<T> *tw, int t, int NS) {
 #pragma unroll
@@ -123,11 +127,20 @@ __device__ __forceinline__ void pass_twiddle(cx<T> (&v)[8], const cx<T> *tw, int
           int j = t + q * (L / 8);
           int jm = j % NS;
           int step = jm * (L / (NS * R));
-#pragma unroll
-          for (int r = 1; r < R; r++) {
-               cx<T> w = twsign<SIGN>(tw[r * step]);
-               v[q + r * (8 / R)] = cmul(v[q + r * (8 / R)], w);
+          cx<T> w[8];
+          w[1] = twsign<SIGN>(tw[step]);
+          if (R >= 4) {
+               w[2] = twsign<SIGN>(tw[2 * step]);
+               w[3] = cmul(w[1], w[2]);
           }
+          if (R == 8) {
+               w[4] = twsign<SIGN>(tw[4 * step]);
+               w[5] = cmul(w[1], w[4]);
+               w[6] = cmul(w[2], w[4]);
+               w[7] = cmul(w[3], w[4]);
+          }
+#pragma unroll
+          for (int r = 1; r < R; r++) v[q + r * (8 / R)] = cmul(v[q + r * (8 / R)], w[r]);
      }
 }
 

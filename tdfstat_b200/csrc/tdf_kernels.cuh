@@ -265,45 +265,89 @@ struct CompSum {
 };
 
 // Split form: phase = het1*i + spnd*i^2 formed and reduced mod 2 pi in FP64,
-// plus spnd*(2 i shft_n[i]) in FP32 per detector; FP32 sincos and products,
-// compensated sum over detectors.
+// plus spnd*(2 i shft_n[i]) in FP32 per detector; FP32 sincos and products.
+// The detector-network sum is compensated (Neumaier) for three or more
+// detectors; for one or two it is a single rounded addition, which the
+// compensation would not change.
 struct DemodSplit {
      const float4 *xab;
      const float *s2;
      const TmplParam *tp;
      int N, N2, Nal, nifo;
+     static constexpr int kQ = 2;   // elements whose operand loads are issued together
+
+     // x * (cs - i sn) for the two arrays of an operand x = (a.re, a.im, b.re, b.im)
+     static __device__ __forceinline__ void rot(const float4 x, float phf, float2 &pa, float2 &pb) {
+          float sn, cs;
+          __sincosf(phf, &sn, &cs);
+          pa = make_float2(fmaf(x.x, cs, x.y * sn), fmaf(x.y, cs, -x.x * sn));
+          pb = make_float2(fmaf(x.z, cs, x.w * sn), fmaf(x.w, cs, -x.z * sn));
+     }
+
      template <int L>
      __device__ __forceinline__ void load(float2 (&v)[2][8], int b, int n2, int t) const {
           const TmplParam P = tp[b];
           const float spf = (float)P.spnd;
           const size_t base = (size_t)P.slot * nifo * Nal;
 #pragma unroll
-          for (int m = 0; m < 8; m++) {
-               const int i = N2 * (t + m * (L / 8)) + n2;
-               float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
-               if (i < N) {
-                    const double di = (double)i;
+          for (int h = 0; h < 8 / kQ; h++) {
+               int ii[kQ];
+               float pr[kQ];
+#pragma unroll
+               for (int q = 0; q < kQ; q++) {
+                    ii[q] = N2 * (t + (kQ * h + q) * (L / 8)) + n2;
+                    const double di = (double)ii[q];
                     const double ph = fma(P.spnd, di * di, P.het1 * di);
                     const double kk = rint(ph * INV_TWO_PI);
-                    const float pr = (float)fma(-kk, TWO_PI, ph);
-                    CompSum ar, ai, br, bi;
-                    for (int d = 0; d < nifo; d++) {
-                         const size_t o = base + (size_t)d * Nal + i;
-                         const float4 x = __ldg(&xab[o]);
-                         const float phf = fmaf(spf, __ldg(&s2[o]), pr);
-                         float sn, cs;
-                         __sincosf(phf, &sn, &cs);
-                         // (x.re + i x.im) * (cs - i sn)
-                         const float pr_ = fmaf(x.x, cs, x.y * sn), pi_ = fmaf(x.y, cs, -x.x * sn);
-                         const float qr_ = fmaf(x.z, cs, x.w * sn), qi_ = fmaf(x.w, cs, -x.z * sn);
-                         if (d == 0) { ar.init(pr_); ai.init(pi_); br.init(qr_); bi.init(qi_); }
-                         else { ar.add(pr_); ai.add(pi_); br.add(qr_); bi.add(qi_); }
-                    }
-                    fa = make_float2(ar.value(), ai.value());
-                    fb = make_float2(br.value(), bi.value());
+                    pr[q] = (float)fma(-kk, TWO_PI, ph);
                }
-               v[0][m] = fa;
-               v[1][m] = fb;
+               float2 fa[kQ], fb[kQ];
+               if (nifo <= 2) {
+                    float4 x0[kQ], x1[kQ];
+                    float s0[kQ], s1[kQ];
+#pragma unroll
+                    for (int q = 0; q < kQ; q++) {
+                         const bool ok = ii[q] < N;
+                         const size_t o = base + ii[q];
+                         x0[q] = ok ? __ldg(&xab[o]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                         s0[q] = ok ? __ldg(&s2[o]) : 0.f;
+                         const bool ok1 = ok && nifo == 2;
+                         x1[q] = ok1 ? __ldg(&xab[o + Nal]) : make_float4(0.f, 0.f, 0.f, 0.f);
+                         s1[q] = ok1 ? __ldg(&s2[o + Nal]) : 0.f;
+                    }
+#pragma unroll
+                    for (int q = 0; q < kQ; q++) {
+                         rot(x0[q], fmaf(spf, s0[q], pr[q]), fa[q], fb[q]);
+                         if (nifo == 2) {
+                              float2 pa, pb;
+                              rot(x1[q], fmaf(spf, s1[q], pr[q]), pa, pb);
+                              fa[q] = cadd(fa[q], pa);
+                              fb[q] = cadd(fb[q], pb);
+                         }
+                    }
+               } else {
+#pragma unroll
+                    for (int q = 0; q < kQ; q++) {
+                         fa[q] = make_float2(0.f, 0.f);
+                         fb[q] = make_float2(0.f, 0.f);
+                         if (ii[q] >= N) continue;
+                         CompSum ar, ai, br, bi;
+                         for (int d = 0; d < nifo; d++) {
+                              const size_t o = base + (size_t)d * Nal + ii[q];
+                              float2 pa, pb;
+                              rot(__ldg(&xab[o]), fmaf(spf, __ldg(&s2[o]), pr[q]), pa, pb);
+                              if (d == 0) { ar.init(pa.x); ai.init(pa.y); br.init(pb.x); bi.init(pb.y); }
+                              else { ar.add(pa.x); ai.add(pa.y); br.add(pb.x); bi.add(pb.y); }
+                         }
+                         fa[q] = make_float2(ar.value(), ai.value());
+                         fb[q] = make_float2(br.value(), bi.value());
+                    }
+               }
+#pragma unroll
+               for (int q = 0; q < kQ; q++) {
+                    v[0][kQ * h + q] = fa[q];
+                    v[1][kQ * h + q] = fb[q];
+               }
           }
      }
 };
@@ -349,13 +393,21 @@ template <typename T> __device__ __forceinline__ T bb_of(const AaBb &ab);
 template <> __device__ __forceinline__ float bb_of<float>(const AaBb &ab) { return ab.bbf; }
 template <> __device__ __forceinline__ double bb_of<double>(const AaBb &ab) { return ab.bb; }
 
-// Row-pass epilogue of the spindown FFT: F[k] over [fr0, fr1]
+// Row-pass epilogue of the spindown FFT: F[k] over [fr0, fr1].  With a
+// candidate list (cand != nullptr) it also appends every bin of the MAX_ALG 3
+// loop range [fr0+1, fr1-2] whose F passes the threshold test, so that the
+// local-maximum rule only has to look at those bins afterwards.
 template <typename T>
 struct StoreFstat {
      T *F;
      const TmplParam *tp;
      const AaBb *ab;
      int nF, fr0, fr1, N1;
+     double thr;
+     uint2 *cand;
+     unsigned *cand_cnt;
+     unsigned cand_cap;
+     int boff;        // index of this chunk's first template within its resolve group
      template <int L>
      __device__ __forceinline__ void store(const cx<T> (&v)[2][8], int b, int k1, int t) const {
           const AaBb s = ab[tp[b].slot];
@@ -364,7 +416,14 @@ struct StoreFstat {
 #pragma unroll
           for (int m = 0; m < 8; m++) {
                const int k = k1 + N1 * (t + m * (L / 8));
-               if (k >= fr0 && k <= fr1) dst[k] = cnorm(v[0][m]) / aa + cnorm(v[1][m]) / bb;
+               if (k >= fr0 && k <= fr1) {
+                    const T f = cnorm(v[0][m]) / aa + cnorm(v[1][m]) / bb;
+                    dst[k] = f;
+                    if (cand && !(f < thr) && k >= fr0 + 1 && k < fr1 - 1) {
+                         const unsigned c = atomicAdd(cand_cnt, 1u);
+                         if (c < cand_cap) cand[c] = make_uint2((unsigned)(b + boff), (unsigned)k);
+                    }
+               }
           }
      }
 };
@@ -404,61 +463,103 @@ __device__ __forceinline__ bool is_peak(const T *Fb, const T *mub, int k, int fr
      return !(f < thr || fval(Fb, mub, k - 1, fr0, nblk) > f || f < fval(Fb, mub, k + 1, fr0, nblk));
 }
 
+struct ThrArgs {
+     int nF, fr0, fr1;
+     double thr;
+     int nblk;
+     const TmplParam *tp;
+     int nfftf;
+     const double *lines;
+     int numlines;
+     unsigned bufhalf;
+     Trig *trig;
+     unsigned long long cap;
+     unsigned long long *cnt;
+     unsigned *tcnt;
+     unsigned *err;
+};
+
 // MAX_ALG 3 (jobcore.c:556-603) as the single-threaded loop executes it:
 // bin i (fr0 < i < fr1-1) is a trigger when it is a local maximum >= thr
 // and the previous accepted bin is not i-1 (the loop's "i++" skip), i.e.
 // when the run of consecutive local-maximum bins ending at i-1 has even
 // length.  Then the veto intervals are checked and the trigger appended.
-// grid (ceil((fr1-fr0+1)/256), ntmpl), 256 threads
 template <typename T, bool FP64>
-__global__ void __launch_bounds__(256) k_threshold(
-     const T *__restrict__ F, int nF, int fr0, int fr1, double thr,
-     const T *__restrict__ mu, int nblk, const TmplParam *__restrict__ tp, int nfftf,
-     const double *__restrict__ lines, int numlines, unsigned bufhalf,
-     Trig *__restrict__ trig, unsigned long long cap, unsigned long long *cnt,
-     unsigned *__restrict__ tcnt, unsigned *err)
+__device__ __forceinline__ void threshold_bin(const T *__restrict__ F, const T *__restrict__ mu, const ThrArgs &A,
+                                              int b, int i)
 {
-     const int b = blockIdx.y;
-     const int i = fr0 + blockIdx.x * 256 + threadIdx.x;
-     if (i < fr0 + 1 || i >= fr1 - 1) return;
-     const T *Fb = F + (size_t)b * nF - fr0;
+     const int fr0 = A.fr0, nblk = A.nblk;
+     const double thr = A.thr;
+     const T *Fb = F + (size_t)b * A.nF - fr0;
      const T *mub = mu ? mu + (size_t)b * nblk : nullptr;
      if (!is_peak(Fb, mub, i, fr0, nblk, thr)) return;
      int run = 0;
      for (int k = i - 1; k >= fr0 + 1 && is_peak(Fb, mub, k, fr0, nblk, thr); k--) run++;
      if (run & 1) return;
      const T Fc = fval(Fb, mub, i, fr0, nblk);
-     const TmplParam P = tp[b];
+     const TmplParam P = A.tp[b];
      double fcmp;
      float ff;
      if (FP64) {
           // FLOAT_TYPE = double: f_ = (double)(2ic)/(double)nfftf*M_PI + sgnl0
-          const double f_ = __dadd_rn(__dmul_rn(__ddiv_rn((double)(2 * i), (double)nfftf), M_PI_D), P.sgnl0);
+          const double f_ = __dadd_rn(__dmul_rn(__ddiv_rn((double)(2 * i), (double)A.nfftf), M_PI_D), P.sgnl0);
           fcmp = f_;
           ff = (float)f_;
      } else {
           // FLOAT_TYPE = float: the quotient in float, the product and sum in
           // double, stored to float
-          const float qf = __fdiv_rn((float)(2 * i), (float)nfftf);
+          const float qf = __fdiv_rn((float)(2 * i), (float)A.nfftf);
           ff = (float)__dadd_rn(__dmul_rn((double)qf, M_PI_D), P.sgnl0);
           fcmp = (double)ff;
      }
-     for (int k = 0; k < numlines; k++)
-          if (fcmp >= lines[2 * k] && fcmp <= lines[2 * k + 1]) return;
-     const unsigned c = atomicAdd(&tcnt[b], 1u);
-     if (c >= bufhalf) {
-          atomicOr(err, ERR_OVERFLOW);
+     for (int k = 0; k < A.numlines; k++)
+          if (fcmp >= A.lines[2 * k] && fcmp <= A.lines[2 * k + 1]) return;
+     const unsigned c = atomicAdd(&A.tcnt[b], 1u);
+     if (c >= A.bufhalf) {
+          atomicOr(A.err, ERR_OVERFLOW);
           return;
      }
-     const unsigned long long g = atomicAdd(cnt, 1ull);
-     if (g < cap) {
+     const unsigned long long g = atomicAdd(A.cnt, 1ull);
+     if (g < A.cap) {
           Trig r;
           r.id = P.id;
           r.bin = (uint32_t)i;
           r.f = ff;
           r.F = (float)Fc;
-          trig[g] = r;
+          A.trig[g] = r;
      }
+}
+
+// The candidates the row pass collected; when the list overflowed, every
+// bin of the chunk (grid-stride).  grid (G), 256 threads
+template <typename T, bool FP64>
+__global__ void __launch_bounds__(256) k_resolve(const T *__restrict__ F, ThrArgs A, const uint2 *__restrict__ cand,
+                                                 const unsigned *__restrict__ cand_cnt, unsigned cand_cap, int nt)
+{
+     const unsigned n = *cand_cnt;
+     const unsigned gs = gridDim.x * blockDim.x;
+     const unsigned g0 = blockIdx.x * blockDim.x + threadIdx.x;
+     if (n <= cand_cap) {
+          for (unsigned c = g0; c < n; c += gs) {
+               const uint2 q = cand[c];
+               threshold_bin<T, FP64>(F, nullptr, A, (int)q.x, (int)q.y);
+          }
+     } else {
+          const unsigned nb = (unsigned)(A.fr1 - A.fr0 - 2 > 0 ? A.fr1 - A.fr0 - 2 : 0);   // bins fr0+1 .. fr1-2
+          for (unsigned long long x = g0; x < (unsigned long long)nt * nb; x += gs)
+               threshold_bin<T, FP64>(F, nullptr, A, (int)(x / nb), A.fr0 + 1 + (int)(x % nb));
+     }
+}
+
+// Full scan of every bin (used with the blocks_avg normalisation).
+// grid (ceil((fr1-fr0+1)/256), ntmpl), 256 threads
+template <typename T, bool FP64>
+__global__ void __launch_bounds__(256) k_threshold(const T *__restrict__ F, const T *__restrict__ mu, ThrArgs A)
+{
+     const int b = blockIdx.y;
+     const int i = A.fr0 + blockIdx.x * 256 + threadIdx.x;
+     if (i < A.fr0 + 1 || i >= A.fr1 - 1) return;
+     threshold_bin<T, FP64>(F, mu, A, b, i);
 }
 
 }  // namespace tdf

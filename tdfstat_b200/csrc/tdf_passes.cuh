@@ -6,8 +6,8 @@
 //     x[N2*n1 + n2] straight into registers (coalesced across the 8 columns),
 //     Epi::store consumes the outputs k1 = t + m*L/8.
 //   k_rowpass<T, L, SIGN, NA, Src, Epi>: CTA = LINES rows k1 of an
-//     N = N1*L transform, L threads; the rows are staged through shared
-//     memory with coalesced loads, Epi::store consumes X[k1 + N1*k2].
+//     N = N1*L transform, L threads; the first-pass inputs are loaded from
+//     the rows straight into registers, Epi::store consumes X[k1 + N1*k2].
 #pragma once
 
 #include "tdf_fft.cuh"
@@ -19,8 +19,14 @@ constexpr size_t pass_smem_bytes() {
      return sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
 }
 
+// resident CTAs per SM the FP32 passes are compiled for (register cap)
+template <typename T, int L>
+constexpr int pass_min_blocks() {
+     return sizeof(T) == 4 ? (L <= 256 ? 3 : (L == 512 ? 2 : 1)) : 1;
+}
+
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
-__global__ void __launch_bounds__(L) k_colpass(Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
+__global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_colpass(Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
      extern __shared__ __align__(16) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
@@ -41,34 +47,28 @@ __global__ void __launch_bounds__(L) k_colpass(Pro pro, Epi epi, const cx<T> *__
 }
 
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
-__global__ void __launch_bounds__(L) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
+__global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
      extern __shared__ __align__(16) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
-     load_table<T>(tw, twline, L);
      const int tid = threadIdx.x;
      const int b = blockIdx.y;
      const int k1b = blockIdx.x * LINES;
-#pragma unroll
-     for (int a = 0; a < NA; a++) {
-          const cx<T> *row0 = src.row(a, b, k1b);
-#pragma unroll 4
-          for (int idx = tid; idx < LINES * L; idx += L) {
-               int row = idx / L, n2 = idx % L;
-               lines[(a * LINES + row) * G::STRIDE + pad8(n2)] = row0[(size_t)row * src.rowstride + n2];
-          }
-     }
-     __syncthreads();
      const int c = tid % LINES, t = tid / LINES;
+     // first-pass inputs straight from the rows into registers: per load
+     // instruction a warp reads 4 consecutive elements of each of 8 rows
+     // (whole 32-byte sectors)
      cx<T> v[NA][8];
      cx<T> *s[NA];
 #pragma unroll
      for (int a = 0; a < NA; a++) {
+          const cx<T> *r = src.row(a, b, k1b + c);
           s[a] = lines + (a * LINES + c) * G::STRIDE;
 #pragma unroll
-          for (int m = 0; m < 8; m++) v[a][m] = s[a][pad8(t + m * (L / 8))];
+          for (int m = 0; m < 8; m++) v[a][m] = r[t + m * (L / 8)];
      }
+     load_table<T>(tw, twline, L);
      __syncthreads();
      line_fft<T, L, SIGN, NA>(v, s, tw, t);
      epi.template store<L>(v, b, k1b + c, t);

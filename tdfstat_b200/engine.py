@@ -120,19 +120,26 @@ class Engine:
         npts = len(pm)
         per = np.zeros(max(npts, 1), dtype=np.int32)
         nrec, npairs = C.c_int64(0), C.c_int64(0)
-        mr = max_recs if max_recs is not None else 0
-        mp = max_pairs if max_pairs is not None else 0
-        for _ in range(2):
+        if max_recs is None:
+            _check(self.lib, self.lib.tdf_count_templates(self.h, npts, _p(pm, C.c_int32), _p(mm, C.c_float),
+                                                          _p(nn, C.c_float), sp, C.byref(nrec), None))
+            mr = nrec.value
+        else:
+            mr = max_recs
+        mp = max_pairs if max_pairs is not None else 8 * mr + 4096
+        recs = (_abi.TdfRecord * max(mr, 1))()
+        pairs = np.empty(max(mp, 1), dtype=np.float32)
+        st = self.lib.tdf_search_points(self.h, npts, _p(pm, C.c_int32), _p(mm, C.c_float), _p(nn, C.c_float), sp,
+                                        recs, mr, C.byref(nrec), _p(pairs, C.c_float), mp, C.byref(npairs),
+                                        _p(per, C.c_int32))
+        if st == _abi.TDF_ERR_CAPACITY and (max_recs is None or max_pairs is None):
+            # the engine kept the results: fetch them into arrays of the right size
+            mr, mp = nrec.value, npairs.value
             recs = (_abi.TdfRecord * max(mr, 1))()
-            pairs = np.zeros(max(mp, 1), dtype=np.float32)
-            st = self.lib.tdf_search_points(self.h, npts, _p(pm, C.c_int32), _p(mm, C.c_float), _p(nn, C.c_float), sp,
-                                            recs, mr, C.byref(nrec), _p(pairs, C.c_float), mp, C.byref(npairs),
-                                            _p(per, C.c_int32))
-            if st == _abi.TDF_ERR_CAPACITY and (max_recs is None or max_pairs is None):
-                mr, mp = nrec.value, npairs.value
-                continue
-            _check(self.lib, st)
-            break
+            pairs = np.empty(max(mp, 1), dtype=np.float32)
+            st = self.lib.tdf_last_results(self.h, recs, mr, C.byref(nrec), _p(pairs, C.c_float), mp,
+                                           C.byref(npairs), _p(per, C.c_int32))
+        _check(self.lib, st)
         n = nrec.value
         a = np.frombuffer(memoryview(recs), dtype=_REC_DTYPE)[:n]
         hdr = np.stack([a["m"], a["n"], a["s"], a["ra"], a["dec"], a["fdot"]], axis=1) if n else np.zeros((0, 6), np.float32)

@@ -1,0 +1,38 @@
+"""The drop-in: the reference's own search host (main.c, init.c, jobcore.c's
+search() loop, compiled unmodified) with job_core() taken from libtdfcuda
+(oracle/_ref/gwsearch-dropin, built by `make -C oracle dropin`).  Its trigger
+files must match the reference's FP64 build (golden records)."""
+import os
+
+import numpy as np
+import pytest
+
+import refkit
+from golden.cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "split": 1e-4}
+
+
+@pytest.mark.parametrize("form", ["fp64", "split"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dropin_matches_reference(golden, name, form):
+    if not os.path.exists(refkit.REF_BIN["dropin"]):
+        pytest.fail("drop-in host not built (make -C oracle dropin)")
+    g = golden(name)
+    import shutil
+    shutil.rmtree(os.path.join(g.root, "out"), ignore_errors=True)
+    from tdfstat_b200 import synth
+    synth.write_case(g.root, g.case)   # restores out/ with the veto-line file
+    recs, meta, out = refkit.run_reference(g.ini, "dropin", threads=4, env={"TDF_FORM": form})
+    ref = g.ref["f64"]
+    assert len(recs) == len(ref)
+    np.testing.assert_array_equal(recs.pm, ref.pm)
+    np.testing.assert_array_equal(recs.hdr[:, :3], ref.hdr[:, :3])
+    r = refkit.compare_records(recs, ref, f_rtol=2e-6 if form == "split" else 1e-12, F_rtol=TOL[form],
+                               thr=g.case.thr, tie_band=TOL[form])
+    assert not r["unmatched"], r["unmatched"][:5]
+    assert r["max_F_rel"] <= TOL[form]
+    assert meta["totsgnl"] == recs.ntrig
+    assert ">>" in out   # the reference's per-sky-point line

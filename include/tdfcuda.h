@@ -166,6 +166,32 @@ int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const f
 int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss,
                        double *F, int64_t nF);
 
+/* F-statistic of one template of the split form from spindown operands that
+   are already on the device, without allocating any memory.  No counterpart
+   in the reference: it is for callers that must not allocate device memory
+   once they run -- hosts whose memory is owned by another allocator or
+   reserved up front, and code paths where the implicit synchronisation of
+   cudaMalloc/cudaFree is not acceptable.  The caller owns every input and
+   output buffer (DEVICE pointers):
+     d_xab : float4 [nifo][Nal]  (xDatma/sig2 re, im, xDatmb/sig2 re, im)
+     d_s2  : float  [nifo][Nal]  (float)(2 i shft[i])
+     d_F   : float  [fr1 - fr0 + 1]  output, F over bins [fr0, fr1]
+   het1, spnd: the template's phase coefficients (FP64); aa, bb: the network
+   sums of the amplitude modulation (jobcore.c:373-386).  The intermediate
+   spectra and FFT tables live in one static device array of the library
+   (about 4.2 MB, held on every GPU that loads the library until the
+   process exits), so nfftf is limited to 2^18 (4096 <= nfftf <= 2^18,
+   power of two, N <= nfftf, 1 <= nifo <= 8); larger sizes are rejected with
+   TDF_ERR_UNSUPPORTED.  The first call on a device resolves the array's
+   device address (and any call with a new nfftf rebuilds the tables in it);
+   make that first call before capturing a stream.  All calls share the one
+   array: calls whose work overlaps on the GPU (other streams, other host
+   threads) race, so serialise them.  Work is enqueued on `stream`
+   (cudaStream_t, NULL = default stream) and completes asynchronously. */
+int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, int32_t nifo, int32_t N, int32_t Nal,
+                              int32_t nfftf, double het1, double spnd, float aa, float bb,
+                              int32_t fr0, int32_t fr1, float *d_F, void *stream);
+
 /* The CUDA stream the engine enqueues on (a cudaStream_t), and a way to make
    it enqueue on the caller's stream instead (NULL = the engine's own). */
 int tdf_engine_get_stream(tdf_engine *e, void **stream);

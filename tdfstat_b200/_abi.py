@@ -124,6 +124,9 @@ ABI_FUNCTIONS = [
      [P, C.c_int, I32P, F32P, F32P, F32P, I64P, I64P]),
     ("tdf_fstat_spectrum", C.c_int,
      [P, C.c_int32, C.c_float, C.c_float, C.c_float, F64P, C.c_int64]),
+    ("tdf_fstat_operands_static", C.c_int,
+     [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_float, C.c_float,
+      C.c_int32, C.c_int32, P, P]),
     ("tdf_engine_get_stream", C.c_int, [P, C.POINTER(P)]),
     ("tdf_engine_set_stream", C.c_int, [P, P]),
     ("tdf_engine_launch_count", C.c_int, [P, I64P]),

@@ -14,6 +14,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -1121,3 +1122,119 @@ int tdf_engine_get_kernel_times(tdf_engine *e, tdf_kernel_times *out) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ allocation-free entry point
+//
+// tdf_fstat_operands_static(): the spindown-stage kernels (column pass with
+// the demodulation, row pass with the F-statistic) of one split-form template
+// on caller-owned device operands.  Its scratch -- the intermediate spectra,
+// the FFT twiddle tables and the template parameters -- is the static array
+// below, so a call allocates nothing.  Host code must not pass the array's
+// name to a kernel (on the host it is only a stand-in); the device address is
+// resolved once per device with cudaGetSymbolAddress.
+
+namespace {
+
+constexpr int kStaticMaxLog2 = 18;                                  // nfftf <= 2^18
+constexpr size_t kStaticY = 2ull * (1ull << kStaticMaxLog2) * sizeof(float2);   // two spectra
+constexpr size_t kStaticTab = (512 + 512 + 256 + 1024) * sizeof(float2);         // line1, line2, hi, lo
+constexpr size_t kStaticPar = 256;                                  // TmplParam + AaBb
+constexpr size_t kStaticBytes = kStaticY + kStaticTab + kStaticPar;
+
+struct StaticDevState {
+     bool ready = false;
+     unsigned char *base = nullptr;   // device address of g_static_scratch on this device
+     int tables_for = 0;              // nfftf the tables currently hold
+};
+constexpr int kStaticMaxDevices = 64;
+StaticDevState g_static_dev[kStaticMaxDevices];
+std::mutex g_static_mu;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+// twiddle tables of an N = N1*N2 transform (forward sign), as FFTTables
+// builds them: line tables of N1 and N2 points, four-step hi/lo tables
+__global__ void k_static_tables(float2 *line1, int N1, float2 *line2, int N2, float2 *hi, float2 *lo, int N)
+{
+     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+     double s, c;
+     if (i < N1) { sincospi(-2.0 * i / N1, &s, &c); line1[i] = make_float2((float)c, (float)s); }
+     if (i < N2) { sincospi(-2.0 * i / N2, &s, &c); line2[i] = make_float2((float)c, (float)s); }
+     if (i < (N >= 1024 ? N / 1024 : 1)) { sincospi(-2.0 * ((double)i * 1024 / N), &s, &c); hi[i] = make_float2((float)c, (float)s); }
+     if (i < 1024) { sincospi(-2.0 * ((double)i / N), &s, &c); lo[i] = make_float2((float)c, (float)s); }
+}
+
+__global__ void k_static_params(TmplParam *tp, AaBb *ab, TmplParam t, AaBb a)
+{
+     if (threadIdx.x == 0 && blockIdx.x == 0) {
+          *tp = t;
+          *ab = a;
+     }
+}
+
+extern "C" int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, int32_t nifo, int32_t N, int32_t Nal,
+                                         int32_t nfftf, double het1, double spnd, float aa, float bb,
+                                         int32_t fr0, int32_t fr1, float *d_F, void *stream)
+{
+     if (!d_xab || !d_s2 || !d_F) return set_error(TDF_ERR_INVALID, "null device pointer");
+     if (nifo < 1 || nifo > TDF_MAX_DETECTORS) return set_error(TDF_ERR_INVALID, "nifo=%d", nifo);
+     if (!pow2(nfftf) || nfftf < 4096)
+          return set_error(TDF_ERR_INVALID, "nfftf=%d must be a power of two >= 4096", nfftf);
+     if (nfftf > (1 << kStaticMaxLog2))
+          return set_error(TDF_ERR_UNSUPPORTED, "nfftf=%d exceeds the static scratch limit 2^%d of tdf_fstat_operands_static",
+                           nfftf, kStaticMaxLog2);
+     if (N < 1 || N > nfftf || Nal < N) return set_error(TDF_ERR_INVALID, "N=%d, Nal=%d, nfftf=%d", N, Nal, nfftf);
+     if (fr0 < 0 || fr1 < fr0 || fr1 >= nfftf) return set_error(TDF_ERR_INVALID, "fr range [%d, %d]", fr0, fr1);
+     if (!(aa > 0.f) || !(bb > 0.f)) return set_error(TDF_ERR_INVALID, "aa, bb must be > 0");
+     int dev = 0;
+     CUCHK(cudaGetDevice(&dev));
+     if (dev < 0 || dev >= kStaticMaxDevices) return set_error(TDF_ERR_UNSUPPORTED, "device %d", dev);
+     cudaStream_t st = (cudaStream_t)stream;
+     const int l = ilog2i(nfftf);
+     const int N1 = 1 << ((l + 1) / 2), N2 = nfftf / N1;
+     unsigned char *base;
+     {
+          std::lock_guard<std::mutex> lk(g_static_mu);
+          StaticDevState &S = g_static_dev[dev];
+          if (!S.ready) {
+               void *p = nullptr;
+               CUCHK(cudaGetSymbolAddress(&p, g_static_scratch));
+               S.base = (unsigned char *)p;
+               S.ready = true;
+          }
+          base = S.base;
+          float2 *tab = (float2 *)(base + kStaticY);
+          if (S.tables_for != nfftf) {
+               k_static_tables<<<(1024 + 255) / 256, 256, 0, st>>>(tab, N1, tab + 512, N2, tab + 1024, tab + 1280, nfftf);
+               CUCHK(cudaGetLastError());
+               S.tables_for = nfftf;
+          }
+     }
+     float2 *Y = (float2 *)base;
+     float2 *tab = (float2 *)(base + kStaticY);
+     const float2 *line1 = tab, *line2 = tab + 512, *hi = tab + 1024, *lo = tab + 1280;
+     TmplParam *tp = (TmplParam *)(base + kStaticY + kStaticTab);
+     AaBb *ab = (AaBb *)(base + kStaticY + kStaticTab + 128);
+     TmplParam t;
+     t.het1 = het1;
+     t.spnd = spnd;
+     t.sgnl0 = 0.;
+     t.slot = 0;
+     t.id = 0;
+     AaBb a;
+     a.aa = aa;
+     a.bb = bb;
+     a.aaf = aa;
+     a.bbf = bb;
+     k_static_params<<<1, 32, 0, st>>>(tp, ab, t, a);
+     CUCHK(cudaGetLastError());
+     DemodSplit pro{(const float4 *)d_xab, d_s2, tp, N, N2, Nal, nifo};
+     StoreFourstep<float, -1, 2> epi{Y, hi, lo, N2, nfftf};
+     TRY((launch_col<float, -1, 2>(N1, dim3(N2 / LINES, 1), pro, epi, line1, st)));
+     RowsY<float, 2> src{Y, nfftf, N2};
+     StoreFstat<float> epi2{d_F, tp, ab, fr1 - fr0 + 1, fr0, fr1, N1, 0.0, nullptr, nullptr, 0u, 0};
+     TRY((launch_row<float, -1, 2>(N2, dim3(N1 / LINES, 1), src, epi2, line2, st)));
+     return TDF_OK;
+}

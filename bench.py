@@ -223,7 +223,9 @@ def run_tdf(args, rank, world, local_rank):
             if world > 1:
                 dist.barrier()
 
-        # warm-up (also compiles nothing: kernels are AOT sm_100a)
+        # chunk size by the engine's autotuner on a 16-point sample (untimed)
+        tuned = eng.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
+        # warm-up (kernels are compiled ahead of time for sm_100a)
         for _ in range(args.warmup):
             eng.search_device(pm, mm, nn)
         torch.cuda.synchronize()
@@ -322,8 +324,8 @@ def run_tdf(args, rank, world, local_rank):
                 "scaling": "weak" if world > 1 else "weak", "vs_baseline": None,
                 "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
                 "data": "synthetic (seeded Gaussian noise + injected CW signal, synthetic ephemeris)",
-                "config": dict(wl.config, form=args.form, l2="flush: 256 MiB write between timed steps; "
-                               "per-step working set > L2"),
+                "config": dict(wl.config, form=args.form, templates_per_chunk=tuned,
+                               l2="flush: 256 MiB write between timed steps; per-step working set > L2"),
                 "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(launches),
@@ -378,6 +380,7 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
     ap.add_argument("--sky-batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--sky-points", type=int, default=0, help="use only the first K sky points (profiling runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

@@ -197,6 +197,14 @@ int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, int32_t nifo
 int tdf_engine_get_stream(tdf_engine *e, void **stream);
 int tdf_engine_set_stream(tdf_engine *e, void *stream);
 
+/* Chooses the templates per chunk of the spindown stage by timing a few
+   sizes (8..32) on these points (device-only passes) and keeps the fastest
+   in the engine; *best (may be NULL) receives it.  With the environment
+   variable TDF_AUTOTUNE_CACHE=<file> the choice is appended to that file and
+   picked up by engines created later for the same form, sizes and GPU. */
+int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
+                        int32_t *best);
+
 /* Kernel launches issued by the engine since creation (for accounting). */
 int tdf_engine_launch_count(tdf_engine *e, int64_t *count);
 

@@ -220,6 +220,7 @@ struct tdf_engine {
      int nF = 0, nblk_mu = 0;
      int Bs = 8;        // sky points per batch
      int Tc = 16;       // templates per chunk (intermediate spectra sized for L2)
+     int TcMax = 32;    // buffers are sized for chunks up to this size
      int64_t launches = 0;
      FFTTables<double> t_nfft, t_ninterp, t_f64;
      FFTTables<float> t_f32;
@@ -356,7 +357,7 @@ static int upload_inputs(tdf_engine *e, const tdf_segment *s) {
 }
 
 static int engine_alloc(tdf_engine *e) {
-     const int nifo = e->nifo, Bs = e->Bs, Tc = e->Tc;
+     const int nifo = e->nifo, Bs = e->Bs, Tc = e->TcMax;
      const size_t Q = (size_t)Bs * nifo;
      TRY(e->xdat.alloc((size_t)nifo * e->Nal * sizeof(float)));
      CUCHK(cudaMemset(e->xdat.p, 0, e->xdat.bytes));
@@ -824,6 +825,55 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
      return TDF_OK;
 }
 
+// ------------------------------------------------------------------ autotuning
+//
+// The templates per chunk (Tc) set how many CTAs a column/row pass launches
+// (32*Tc and 64*Tc for nfftf = 2^17) against the SM count, and how much of
+// L2 the intermediate spectra take.  tdf_engine_autotune() times candidates
+// on the caller's points; with TDF_AUTOTUNE_CACHE=<file> the choice is kept
+// per (form, N, nfftf, nifo, SM count, sky batch) and reused by later
+// engines.
+
+static int sm_count(int dev) {
+     int n = 0;
+     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+          cudaGetLastError();
+          return 0;
+     }
+     return n;
+}
+
+static std::string autotune_key(const tdf_engine *e) {
+     char k[256];
+     snprintf(k, sizeof(k), "tc %d %d %d %d %d %d", e->form, e->N, e->nfftf, e->nifo, sm_count(e->dev), e->Bs);
+     return k;
+}
+
+static void autotune_cache_lookup(tdf_engine *e) {
+     const char *path = getenv("TDF_AUTOTUNE_CACHE");
+     if (!path || !*path || getenv("TDF_TEMPLATES_PER_CHUNK")) return;
+     FILE *f = fopen(path, "r");
+     if (!f) return;
+     const std::string key = autotune_key(e);
+     char line[512];
+     while (fgets(line, sizeof(line), f)) {
+          if (strncmp(line, key.c_str(), key.size()) == 0 && line[key.size()] == ' ') {
+               int tc = atoi(line + key.size() + 1);
+               if (tc > 0 && tc <= e->TcMax) e->Tc = tc;
+          }
+     }
+     fclose(f);
+}
+
+static void autotune_cache_store(const tdf_engine *e) {
+     const char *path = getenv("TDF_AUTOTUNE_CACHE");
+     if (!path || !*path) return;
+     FILE *f = fopen(path, "a");
+     if (!f) return;
+     fprintf(f, "%s %d\n", autotune_key(e).c_str(), e->Tc);
+     fclose(f);
+}
+
 // ------------------------------------------------------------------ C ABI
 
 extern "C" {
@@ -890,6 +940,8 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (max_sky_batch > 0) e->Bs = max_sky_batch;
      const char *tc = getenv("TDF_TEMPLATES_PER_CHUNK");
      if (tc && atoi(tc) > 0) e->Tc = atoi(tc);
+     e->TcMax = std::max(32, e->Tc);
+     autotune_cache_lookup(e);
      e->lines.assign(opts->lines, opts->lines + 2 * (size_t)opts->numlines);
      e->opts.lines = nullptr;
      e->dets.resize(seg->nifo);
@@ -1093,6 +1145,51 @@ int tdf_engine_set_stream(tdf_engine *e, void *stream) {
      CUCHK(cudaSetDevice(e->dev));
      CUCHK(cudaStreamSynchronize(e->stream));
      e->stream = stream ? (cudaStream_t)stream : e->own;
+     return TDF_OK;
+}
+
+int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
+                        int32_t *best) {
+     if (!e) return set_error(TDF_ERR_INVALID, "null engine");
+     CUCHK(cudaSetDevice(e->dev));
+     static const int cands[] = {8, 12, 16, 20, 24, 28, 32};
+     cudaEvent_t a, b;
+     CUCHK(cudaEventCreate(&a));
+     CUCHK(cudaEventCreate(&b));
+     const int keep = e->Tc;
+     double best_ms = 1e300;
+     int best_tc = keep;
+     std::vector<HostPoint> pts;
+     std::vector<HostTmpl> tm;
+     int64_t ntrig = 0;
+     int st = TDF_OK;
+     for (int c : cands) {
+          if (c > e->TcMax) continue;
+          e->Tc = c;
+          float ms = 0.f, m2 = 1e30f;
+          for (int rep = 0; rep < 2 && st == TDF_OK; rep++) {
+               cudaEventRecord(a, e->stream);
+               st = search_core(e, npts, pm, mm, nn, nullptr, pts, tm, false, &ntrig);
+               cudaEventRecord(b, e->stream);
+               cudaEventSynchronize(b);
+               cudaEventElapsedTime(&ms, a, b);
+               m2 = std::min(m2, ms);
+          }
+          if (st != TDF_OK) break;
+          if (m2 < best_ms) {
+               best_ms = m2;
+               best_tc = c;
+          }
+     }
+     cudaEventDestroy(a);
+     cudaEventDestroy(b);
+     if (st != TDF_OK) {
+          e->Tc = keep;
+          return st;
+     }
+     e->Tc = best_tc;
+     autotune_cache_store(e);
+     if (best) *best = best_tc;
      return TDF_OK;
 }
 

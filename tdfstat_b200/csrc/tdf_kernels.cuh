@@ -274,7 +274,7 @@ struct DemodSplit {
      const float *s2;
      const TmplParam *tp;
      int N, N2, Nal, nifo;
-     static constexpr int kQ = 2;   // elements whose operand loads are issued together
+     static constexpr int kQ = 1;   // elements whose operand loads are issued together
 
      // x * (cs - i sn) for the two arrays of an operand x = (a.re, a.im, b.re, b.im)
      static __device__ __forceinline__ void rot(const float4 x, float phf, float2 &pa, float2 &pb) {
@@ -294,14 +294,25 @@ struct DemodSplit {
                int ii[kQ];
                float pr[kQ];
 #pragma unroll
+               for (int q = 0; q < kQ; q++) ii[q] = N2 * (t + (kQ * h + q) * (L / 8)) + n2;
+               float2 fa[kQ], fb[kQ];
+               if (ii[0] >= N) {
+                    // zero padding beyond N: the whole group (the tail rows of
+                    // every column, uniform across the warp)
+#pragma unroll
+                    for (int q = 0; q < kQ; q++) {
+                         v[0][kQ * h + q] = make_float2(0.f, 0.f);
+                         v[1][kQ * h + q] = make_float2(0.f, 0.f);
+                    }
+                    continue;
+               }
+#pragma unroll
                for (int q = 0; q < kQ; q++) {
-                    ii[q] = N2 * (t + (kQ * h + q) * (L / 8)) + n2;
                     const double di = (double)ii[q];
                     const double ph = fma(P.spnd, di * di, P.het1 * di);
                     const double kk = rint(ph * INV_TWO_PI);
                     pr[q] = (float)fma(-kk, TWO_PI, ph);
                }
-               float2 fa[kQ], fb[kQ];
                if (nifo <= 2) {
                     float4 x0[kQ], x1[kQ];
                     float s0[kQ], s1[kQ];
@@ -317,6 +328,11 @@ struct DemodSplit {
                     }
 #pragma unroll
                     for (int q = 0; q < kQ; q++) {
+                         if (ii[q] >= N) {
+                              fa[q] = make_float2(0.f, 0.f);
+                              fb[q] = make_float2(0.f, 0.f);
+                              continue;
+                         }
                          rot(x0[q], fmaf(spf, s0[q], pr[q]), fa[q], fb[q]);
                          if (nifo == 2) {
                               float2 pa, pb;

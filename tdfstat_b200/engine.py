@@ -172,6 +172,16 @@ class Engine:
     def set_stream(self, stream_ptr: int):
         _check(self.lib, self.lib.tdf_engine_set_stream(self.h, C.c_void_p(stream_ptr)))
 
+    def autotune(self, pm, mm, nn) -> int:
+        """Times chunk sizes on these points and keeps the fastest."""
+        pm = np.ascontiguousarray(pm, dtype=np.int32)
+        mm = np.ascontiguousarray(mm, dtype=np.float32)
+        nn = np.ascontiguousarray(nn, dtype=np.float32)
+        best = C.c_int32(0)
+        _check(self.lib, self.lib.tdf_engine_autotune(self.h, len(pm), _p(pm, C.c_int32), _p(mm, C.c_float),
+                                                      _p(nn, C.c_float), C.byref(best)))
+        return best.value
+
     def enable_kernel_timing(self, on: bool = True):
         _check(self.lib, self.lib.tdf_engine_set_kernel_timing(self.h, 1 if on else 0))
 

@@ -163,13 +163,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per template of the dominant kernel from the committed ncu
-    summary (profiles/traffic.json), if present."""
-    p = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
+def profile_traffic(workload: str, form: str):
+    """DRAM bytes per template of the column pass, from the committed ncu
+    summary profiles/traffic_<workload>_<form>.md (its k_colpass table row),
+    or None when there is no summary for this workload and form."""
+    p = os.path.join(REPO, "profiles", "traffic_%s_%s.md" % (workload, form))
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if cells and cells[0] == "k_colpass" and len(cells) >= 6:
+                return float(cells[5].split()[0])
     return None
 
 
@@ -297,10 +302,8 @@ def run_tdf(args, rank, world, local_rank):
                 per_launch_bytes = bt * col_t / col_n
                 avg_s = col_ms / col_n / 1e3
                 achieved = per_launch_bytes / avg_s / 1e9
-                tr = profile_traffic()
-                traffic = None
-                if tr and tr.get("workload") == args.workload and tr.get("form") == args.form:
-                    traffic = tr["dram_bytes_per_template"] * col_t / col_n
+                tr = profile_traffic(args.workload, args.form)
+                traffic = round(tr * col_t / col_n) if tr is not None else None
                 roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 4), "traffic": traffic,
                         "kernel": "k_colpass (demodulation + first FFT pass)",

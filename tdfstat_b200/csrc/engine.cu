@@ -212,6 +212,9 @@ struct HostPoint {
 struct tdf_engine {
      int dev = 0, form = TDF_FORM_SPLIT;
      cudaStream_t own = nullptr, stream = nullptr;
+     cudaStream_t sky_stream = nullptr;   // sky stage of the next batch runs here, overlapping
+     bool overlap = false;                // true: sky stage on its own stream (TDF_SKY_OVERLAP=1)
+     cudaEvent_t sky_done[2] = {nullptr, nullptr}, spin_done[2] = {nullptr, nullptr};
      tdf_segment seg{};
      tdf_search_opts opts{};
      std::vector<double> lines;
@@ -227,9 +230,9 @@ struct tdf_engine {
      // inputs
      DevBuf xdat, detssb, cosm, sinm, pco, gco, detp;
      // sky stage
-     DevBuf skyp, B0, B1, B2, shftf, partial, aabb;
+     DevBuf skyp[2], B0, B1, B2, shftf, partial, aabb[2];
      // operands
-     DevBuf xab, s2, xa64, xb64, t1;
+     DevBuf xab[2], s2[2], xa64[2], xb64[2], t1[2];   // per batch slot
      // spindown stage
      DevBuf tparam, Ybuf, Fbuf, mubuf, tcnt, linesd, cand;
      unsigned cand_cap = 0;
@@ -262,7 +265,7 @@ enum { KT_COL = 0, KT_ROW = 1, KT_THR = 2, KT_SKY = 3 };
 
 // records the opening event of a timed region; returns the index of an
 // event pair in the pool (pairs are recycled once collected)
-static size_t timing_begin(tdf_engine *e) {
+static size_t timing_begin(tdf_engine *e, cudaStream_t st = nullptr) {
      if (e->evfree.empty()) {
           cudaEvent_t a, b;
           if (cudaEventCreate(&a) != cudaSuccess) return (size_t)-1;
@@ -276,13 +279,13 @@ static size_t timing_begin(tdf_engine *e) {
      }
      size_t i = e->evfree.back();
      e->evfree.pop_back();
-     cudaEventRecord(e->evpool[i], e->stream);
+     cudaEventRecord(e->evpool[i], st ? st : e->stream);
      return i;
 }
 
-static void timing_end(tdf_engine *e, size_t i, int kind, int64_t templates) {
+static void timing_end(tdf_engine *e, size_t i, int kind, int64_t templates, cudaStream_t st = nullptr) {
      if (i == (size_t)-1) return;
-     cudaEventRecord(e->evpool[i + 1], e->stream);
+     cudaEventRecord(e->evpool[i + 1], st ? st : e->stream);
      e->pending.push_back({kind, i, templates});
 }
 
@@ -378,22 +381,26 @@ static int engine_alloc(tdf_engine *e) {
           CUCHK(cudaMemcpy(e->pco.p, p.data(), n * sizeof(double), cudaMemcpyHostToDevice));
           CUCHK(cudaMemcpy(e->gco.p, g.data(), n * sizeof(double), cudaMemcpyHostToDevice));
      }
-     TRY(e->skyp.alloc(Bs * sizeof(SkyParam)));
+     for (int k = 0; k < 2; k++) TRY(e->skyp[k].alloc(Bs * sizeof(SkyParam)));
      const size_t ws = Wstride(e);
      TRY(e->B0.alloc(Q * 2 * ws * sizeof(double2)));
      TRY(e->B1.alloc(Q * 2 * ws * sizeof(double2)));
      TRY(e->B2.alloc(Q * 2 * ws * sizeof(double2)));
      TRY(e->shftf.alloc(Q * e->Nal * sizeof(double)));
      TRY(e->partial.alloc(Q * (e->nfft / 256) * 2 * sizeof(double)));
-     TRY(e->aabb.alloc(Bs * sizeof(AaBb)));
+     for (int k = 0; k < 2; k++) TRY(e->aabb[k].alloc(Bs * sizeof(AaBb)));
      const size_t ops = Q * e->Nal;
      if (e->form == TDF_FORM_SPLIT) {
-          TRY(e->xab.alloc(ops * sizeof(float4)));
-          TRY(e->s2.alloc(ops * sizeof(float)));
+          for (int k = 0; k < 2; k++) {
+               TRY(e->xab[k].alloc(ops * sizeof(float4)));
+               TRY(e->s2[k].alloc(ops * sizeof(float)));
+          }
      } else {
-          TRY(e->xa64.alloc(ops * sizeof(double2)));
-          TRY(e->xb64.alloc(ops * sizeof(double2)));
-          TRY(e->t1.alloc(ops * sizeof(double)));
+          for (int k = 0; k < 2; k++) {
+               TRY(e->xa64[k].alloc(ops * sizeof(double2)));
+               TRY(e->xb64[k].alloc(ops * sizeof(double2)));
+               TRY(e->t1[k].alloc(ops * sizeof(double)));
+          }
      }
      const size_t csz = e->form == TDF_FORM_SPLIT ? sizeof(float2) : sizeof(double2);
      const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
@@ -424,9 +431,10 @@ static int engine_alloc(tdf_engine *e) {
 }
 
 static void engine_free(tdf_engine *e) {
-     DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp,
-                       &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb, &e->xab, &e->s2,
-                       &e->xa64, &e->xb64, &e->t1, &e->tparam, &e->Ybuf, &e->Fbuf, &e->mubuf,
+     DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp[0],
+                       &e->skyp[1], &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb[0], &e->aabb[1],
+                       &e->xab[0], &e->xab[1], &e->s2[0], &e->s2[1], &e->xa64[0], &e->xa64[1], &e->xb64[0],
+                       &e->xb64[1], &e->t1[0], &e->t1[1], &e->tparam, &e->Ybuf, &e->Fbuf, &e->mubuf,
                        &e->trig[0], &e->trig[1], &e->counters[0], &e->counters[1], &e->tcnt, &e->linesd, &e->cand};
      for (DevBuf *b : bufs) b->release();
      e->t_nfft.release();
@@ -447,6 +455,13 @@ static void engine_free(tdf_engine *e) {
      e->evpool.clear();
      e->evfree.clear();
      e->pending.clear();
+     for (int k = 0; k < 2; k++) {
+          if (e->sky_done[k]) cudaEventDestroy(e->sky_done[k]);
+          if (e->spin_done[k]) cudaEventDestroy(e->spin_done[k]);
+          e->sky_done[k] = e->spin_done[k] = nullptr;
+     }
+     if (e->sky_stream) cudaStreamDestroy(e->sky_stream);
+     e->sky_stream = nullptr;
      if (e->own) cudaStreamDestroy(e->own);
      e->own = nullptr;
 }
@@ -522,21 +537,26 @@ static float rec_fdot(const tdf_engine *e, double spnd) {
 
 // ------------------------------------------------------------------ device pipeline
 
+// Sky stage of npts points into batch slot e->cur, on the sky stream: it
+// first waits until the slot's previous spindown work released the slot's
+// operands, and records sky_done[slot] for the spindown work to wait on.
 static int run_sky_stage(tdf_engine *e, int npts) {
-     cudaStream_t st = e->stream;
+     cudaStream_t st = e->overlap ? e->sky_stream : e->stream;
+     CUCHK(cudaStreamWaitEvent(st, e->spin_done[e->cur], 0));
      const int nifo = e->nifo, Q = npts * nifo;
      const size_t ws = Wstride(e);
-     CUCHK(cudaMemcpyAsync(e->skyp.p, e->h_sky[e->cur], npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
+     const int sl = e->cur;
+     CUCHK(cudaMemcpyAsync(e->skyp[sl].p, e->h_sky[sl], npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
      const int nblk = e->nfft / 256;
      const bool split = e->form == TDF_FORM_SPLIT;
      k_sky_prep<<<dim3(nblk, Q), 256, 0, st>>>(
           e->xdat.as<float>(), e->detssb.as<double>(), e->cosm.as<double>(), e->sinm.as<double>(),
-          e->skyp.as<SkyParam>(), e->detp.as<DetParam>(), nifo, e->N, e->nfft, e->Nal, e->seg.oms,
-          e->B0.as<double2>(), ws, e->shftf.as<double>(), split ? e->s2.as<float>() : nullptr,
-          split ? nullptr : e->t1.as<double>(), e->partial.as<double>());
+          e->skyp[sl].as<SkyParam>(), e->detp.as<DetParam>(), nifo, e->N, e->nfft, e->Nal, e->seg.oms,
+          e->B0.as<double2>(), ws, e->shftf.as<double>(), split ? e->s2[sl].as<float>() : nullptr,
+          split ? nullptr : e->t1[sl].as<double>(), e->partial.as<double>());
      CUCHK(cudaGetLastError());
-     k_sky_sums<<<(npts + 31) / 32, 32, 0, st>>>(e->partial.as<double>(), nblk, e->detp.as<DetParam>(), nifo, npts,
-                                                   e->aabb.as<AaBb>());
+     k_sky_sums<<<npts, 256, 0, st>>>(e->partial.as<double>(), nblk, e->detp.as<DetParam>(), nifo,
+                                       e->aabb[sl].as<AaBb>());
      CUCHK(cudaGetLastError());
      e->launches += 2;
      // forward FFT (nfft) of every (point, detector, a|b): B0 -> B1 -> B2
@@ -564,7 +584,7 @@ static int run_sky_stage(tdf_engine *e, int npts) {
      e->launches += 4;
      // spline: B0 (samples) -> B1 (u) -> B2 (second derivatives)
      {
-          const int K = 128, Wu = 48;
+          const int K = 64, Wu = 48;   // chunk per thread, warm-up steps
           const int nch = (e->n2N + K - 1) / K;
           dim3 g((nch + 127) / 128, 2 * Q);
           k_spline_fwd<<<g, 128, 0, st>>>(e->B0.as<double2>(), e->B1.as<double2>(), ws, e->pco.as<double>(), e->n2N, K, Wu);
@@ -574,10 +594,11 @@ static int run_sky_stage(tdf_engine *e, int npts) {
      }
      k_splint<<<dim3((e->N + 255) / 256, Q), 256, 0, st>>>(
           e->B0.as<double2>(), e->B2.as<double2>(), ws, e->shftf.as<double>(), e->Nal, e->N, e->n2N,
-          e->seg.interpftpad, e->detp.as<DetParam>(), nifo, split ? e->xab.as<float4>() : nullptr,
-          split ? nullptr : e->xa64.as<double2>(), split ? nullptr : e->xb64.as<double2>());
+          e->seg.interpftpad, e->detp.as<DetParam>(), nifo, split ? e->xab[sl].as<float4>() : nullptr,
+          split ? nullptr : e->xa64[sl].as<double2>(), split ? nullptr : e->xb64[sl].as<double2>());
      CUCHK(cudaGetLastError());
      e->launches += 3;
+     CUCHK(cudaEventRecord(e->sky_done[sl], st));
      return TDF_OK;
 }
 
@@ -598,16 +619,17 @@ static int run_chunk(tdf_engine *e, const TmplParam *dtp, int ci, int nt) {
      StoreFourstep<T, -1, 2> epi{e->Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
      size_t tev = e->timing ? timing_begin(e) : (size_t)-1;
      if constexpr (std::is_same<T, float>::value) {
-          DemodSplit pro{e->xab.as<float4>(), e->s2.as<float>(), ctp, e->N, t.N2, e->Nal, e->nifo};
+          DemodSplit pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal, e->nifo};
           TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
      } else {
-          DemodFP64 pro{e->xa64.as<double2>(), e->xb64.as<double2>(), e->t1.as<double>(), ctp, e->N, t.N2, e->Nal, e->nifo};
+          DemodFP64 pro{e->xa64[e->cur].as<double2>(), e->xb64[e->cur].as<double2>(), e->t1[e->cur].as<double>(), ctp,
+                        e->N, t.N2, e->Nal, e->nifo};
           TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
      }
      if (e->timing) timing_end(e, tev, KT_COL, nt);
      const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
      RowsY<T, 2> src{e->Ybuf.as<cx<T>>(), e->nfftf, t.N2};
-     StoreFstat<T> epi2{e->Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb.as<AaBb>(), e->nF, e->opts.fr[0],
+     StoreFstat<T> epi2{e->Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF, e->opts.fr[0],
                         e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : e->cand.as<uint2>(), tcnt + G,
                         e->cand_cap, boff};
      tev = e->timing ? timing_begin(e) : (size_t)-1;
@@ -728,21 +750,19 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
      if (npts < 0) return set_error(TDF_ERR_INVALID, "npts < 0");
      if (npts > 0 && (!pm || !mm || !nn)) return set_error(TDF_ERR_INVALID, "null sky point arrays");
      pts.assign(npts, HostPoint());
-     tm.clear();
+     // the point geometry up front (cheap); the per-template scalars are made
+     // batch by batch below, while the device runs the previous batch
+     int64_t ntm = 0;
      for (int i = 0; i < npts; i++) {
           if (pm[i] != 1 && pm[i] != 2) return set_error(TDF_ERR_INVALID, "pm[%d]=%d (must be 1 or 2)", i, pm[i]);
           float s0 = sst ? sst[i] : e->opts.spndr[0];
           point_setup(e, pm[i], mm[i], nn[i], s0, pts[i]);
           if (!pts[i].inside) continue;
-          pts[i].first_tmpl = (int)tm.size();
-          for (int iss = 0; iss < pts[i].iss_size; iss++) {
-               HostTmpl T;
-               T.pt = i;
-               float ss = pts[i].smin + iss * e->opts.sstep;
-               tmpl_setup(e, pts[i], mm[i], nn[i], ss, T);
-               tm.push_back(T);
-          }
+          pts[i].first_tmpl = (int)ntm;
+          ntm += pts[i].iss_size;
      }
+     if (ntm > (int64_t)UINT32_MAX) return set_error(TDF_ERR_UNSUPPORTED, "more than 2^32 templates in one call");
+     tm.resize(ntm);
      // sky batches of consecutive inside points
      std::vector<int> inside;
      for (int i = 0; i < npts; i++)
@@ -757,6 +777,7 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
      for (int attempt = 0;; attempt++) {
           e->h_trig.clear();
           *ntrig_total = 0;
+          CUCHK(cudaStreamSynchronize(e->sky_stream));
           CUCHK(cudaStreamSynchronize(e->stream));
           for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
           CUCHK(cudaMemsetAsync(e->tcnt.p, 0, e->tcnt.bytes, e->stream));
@@ -782,9 +803,12 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
                }
                int w = 0;
                for (int k = 0; k < nb; k++) {
-                    const HostPoint &P = pts[inside[b0 + k]];
+                    const int ip = inside[b0 + k];
+                    const HostPoint &P = pts[ip];
                     for (int s = 0; s < P.iss_size; s++) {
-                         const HostTmpl &T = tm[P.first_tmpl + s];
+                         HostTmpl &T = tm[P.first_tmpl + s];
+                         T.pt = ip;
+                         tmpl_setup(e, P, mm[ip], nn[ip], P.smin + s * e->opts.sstep, T);
                          TmplParam &q = e->h_tp[slot][w++];
                          q.het1 = T.het1;
                          q.spnd = T.spnd;
@@ -793,11 +817,14 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
                          q.id = (uint32_t)(P.first_tmpl + s);
                     }
                }
-               size_t sev = e->timing ? timing_begin(e) : (size_t)-1;
+               cudaStream_t sst = e->overlap ? e->sky_stream : e->stream;
+               size_t sev = e->timing ? timing_begin(e, sst) : (size_t)-1;
                TRY(run_sky_stage(e, nb));
-               if (e->timing) timing_end(e, sev, KT_SKY, nb);
+               if (e->timing) timing_end(e, sev, KT_SKY, nb, sst);
+               CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[slot], 0));
                CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[slot], nt * sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
                TRY(run_templates(e, e->tparam.as<TmplParam>(), nt));
+               CUCHK(cudaEventRecord(e->spin_done[slot], e->stream));
                CUCHK(cudaMemcpyAsync(e->h_cnt + 2 * slot, e->counters[slot].p, 2 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, e->stream));
                CUCHK(cudaEventRecord(e->done[slot], e->stream));
@@ -940,13 +967,20 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (max_sky_batch > 0) e->Bs = max_sky_batch;
      const char *tc = getenv("TDF_TEMPLATES_PER_CHUNK");
      if (tc && atoi(tc) > 0) e->Tc = atoi(tc);
-     e->TcMax = std::max(32, e->Tc);
+     e->TcMax = std::max(48, e->Tc);
+     const char *ov = getenv("TDF_SKY_OVERLAP");
+     e->overlap = ov && atoi(ov) != 0;   // measured: off is faster when the spindown kernels fill the GPU
      autotune_cache_lookup(e);
      e->lines.assign(opts->lines, opts->lines + 2 * (size_t)opts->numlines);
      e->opts.lines = nullptr;
      e->dets.resize(seg->nifo);
      int st = TDF_OK;
      cudaError_t ce = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking);
+     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->sky_stream, cudaStreamNonBlocking);
+     for (int k = 0; k < 2 && ce == cudaSuccess; k++) {
+          ce = cudaEventCreateWithFlags(&e->sky_done[k], cudaEventDisableTiming);
+          if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->spin_done[k], cudaEventDisableTiming);
+     }
      if (ce != cudaSuccess) st = set_error(TDF_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(ce));
      e->stream = e->own;
      if (st == TDF_OK) st = engine_alloc(e);
@@ -973,13 +1007,16 @@ int tdf_engine_upload(tdf_engine *e, const tdf_segment *seg) {
          seg->nifo != e->nifo)
           return set_error(TDF_ERR_INVALID, "segment sizes differ from the engine's");
      CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->sky_stream));
      TRY(upload_inputs(e, seg));
+     CUCHK(cudaStreamSynchronize(e->stream));
      return TDF_OK;
 }
 
 int tdf_engine_destroy(tdf_engine *e) {
      if (!e) return TDF_OK;
      cudaSetDevice(e->dev);
+     if (e->sky_stream) cudaStreamSynchronize(e->sky_stream);
      if (e->stream) cudaStreamSynchronize(e->stream);
      engine_free(e);
      delete e;
@@ -1100,6 +1137,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      if (!P.inside) return set_error(TDF_ERR_INVALID, "sky point outside the grid ellipse");
      HostTmpl T;
      tmpl_setup(e, P, mm, nn, ss, T);
+     CUCHK(cudaStreamSynchronize(e->sky_stream));
      CUCHK(cudaStreamSynchronize(e->stream));
      TRY(ensure_tparam(e, 1));
      e->cur = 0;
@@ -1111,6 +1149,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      q.slot = 0;
      q.id = 0;
      TRY(run_sky_stage(e, 1));
+     CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[0], 0));
      CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[0], sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
      CUCHK(cudaMemsetAsync(e->counters[0].p, 0, 2 * sizeof(unsigned long long), e->stream));
      CUCHK(cudaMemsetAsync(e->tcnt.p, 0, e->tcnt.bytes, e->stream));
@@ -1152,7 +1191,7 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
                         int32_t *best) {
      if (!e) return set_error(TDF_ERR_INVALID, "null engine");
      CUCHK(cudaSetDevice(e->dev));
-     static const int cands[] = {8, 12, 16, 20, 24, 28, 32};
+     static const int cands[] = {8, 12, 16, 20, 24, 28, 32, 37, 41, 48};
      cudaEvent_t a, b;
      CUCHK(cudaEventCreate(&a));
      CUCHK(cudaEventCreate(&b));

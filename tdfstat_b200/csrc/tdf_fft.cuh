@@ -118,10 +118,12 @@ template <typename T, int L> struct LineGeom {
 constexpr int LINES = 8;   // lines (columns or rows) per CTA
 
 // Apply the Stockham twiddles of a pass (radix R, span NS) to the butterflies
-// a thread owns.  tw[m] = e^{-2 pi i m / L}, m < L (shared memory).  Powers
-// 1, 2, 4 come from the table, the others as products of two of them.
-template <typename T, int L, int R, int SIGN>
-__device__ __forceinline__ void pass_twiddle(cx<T> (&v)[8], const cx<T> *tw, int t, int NS) {
+// a thread owns, for all NA lines it holds (the twiddles depend only on the
+// butterfly, so they are formed once).  tw[m] = e^{-2 pi i m / L}, m < L
+// (shared memory).  Powers 1, 2, 4 come from the table, the others as
+// products of two of them.
+template <typename T, int L, int R, int SIGN, int NA>
+__device__ __forceinline__ void pass_twiddle(cx<T> (&v)[NA][8], const cx<T> *tw, int t, int NS) {
 #pragma unroll
      for (int q = 0; q < 8 / R; q++) {
           int j = t + q * (L / 8);
@@ -140,7 +142,10 @@ __device__ __forceinline__ void pass_twiddle(cx<T> (&v)[8], const cx<T> *tw, int
                w[7] = cmul(w[3], w[4]);
           }
 #pragma unroll
-          for (int r = 1; r < R; r++) v[q + r * (8 / R)] = cmul(v[q + r * (8 / R)], w[r]);
+          for (int a = 0; a < NA; a++) {
+#pragma unroll
+               for (int r = 1; r < R; r++) v[a][q + r * (8 / R)] = cmul(v[a][q + r * (8 / R)], w[r]);
+          }
      }
 }
 
@@ -189,10 +194,7 @@ __device__ __forceinline__ void line_fft(cx<T> (&v)[NA][8], cx<T> *const (&s)[NA
      int NS = 1;
 #pragma unroll
      for (int p = 0; p < G::P8; p++) {
-          if (p > 0) {
-#pragma unroll
-               for (int a = 0; a < NA; a++) pass_twiddle<T, L, 8, SIGN>(v[a], tw, t, NS);
-          }
+          if (p > 0) pass_twiddle<T, L, 8, SIGN, NA>(v, tw, t, NS);
 #pragma unroll
           for (int a = 0; a < NA; a++) pass_dft<8, SIGN>(v[a]);
           const bool last = (p == G::P8 - 1) && (G::RL == 1);
@@ -214,11 +216,9 @@ __device__ __forceinline__ void line_fft(cx<T> (&v)[NA][8], cx<T> *const (&s)[NA
      }
      if (G::RL > 1) {
           constexpr int RR = G::RL > 1 ? G::RL : 2;
+          pass_twiddle<T, L, RR, SIGN, NA>(v, tw, t, NS);
 #pragma unroll
-          for (int a = 0; a < NA; a++) {
-               pass_twiddle<T, L, RR, SIGN>(v[a], tw, t, NS);
-               pass_dft<RR, SIGN>(v[a]);
-          }
+          for (int a = 0; a < NA; a++) pass_dft<RR, SIGN>(v[a]);
      }
 }
 

@@ -135,28 +135,45 @@ __global__ void __launch_bounds__(256) k_sky_prep(
      }
 }
 
-// one thread per sky point: aa = sum_n sum_i aa_n^2/sig2_n (jobcore.c:373-386),
-// accumulated per detector into FLOAT_TYPE as the reference build does
-__global__ void k_sky_sums(const double *__restrict__ partial, int nblk, const DetParam *__restrict__ dp,
-                           int nifo, int npts, AaBb *__restrict__ out)
+// one CTA per sky point: aa = sum_n sum_i aa_n^2/sig2_n (jobcore.c:373-386);
+// each detector's partials reduced by a fixed tree (reproducible), then
+// accumulated over detectors into FLOAT_TYPE as the reference build does.
+// grid (npts), 256 threads
+__global__ void __launch_bounds__(256) k_sky_sums(const double *__restrict__ partial, int nblk,
+                                                  const DetParam *__restrict__ dp, int nifo, AaBb *__restrict__ out)
 {
-     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-     if (p >= npts) return;
+     const int p = blockIdx.x;
+     __shared__ double ra[256], rb[256];
      double aa = 0., bb = 0.;
      float aaf = 0.f, bbf = 0.f;
      for (int d = 0; d < nifo; d++) {
           const double *pp = partial + (size_t)(p * nifo + d) * nblk * 2;
           double sa = 0., sb = 0.;
-          for (int k = 0; k < nblk; k++) { sa += pp[2 * k]; sb += pp[2 * k + 1]; }
+          for (int k = threadIdx.x; k < nblk; k += 256) { sa += pp[2 * k]; sb += pp[2 * k + 1]; }
+          ra[threadIdx.x] = sa;
+          rb[threadIdx.x] = sb;
+          __syncthreads();
+          for (int o = 128; o > 0; o >>= 1) {
+               if (threadIdx.x < o) {
+                    ra[threadIdx.x] += ra[threadIdx.x + o];
+                    rb[threadIdx.x] += rb[threadIdx.x + o];
+               }
+               __syncthreads();
+          }
+          sa = ra[0];
+          sb = rb[0];
+          __syncthreads();
           aa += sa / dp[d].sig2;
           bb += sb / dp[d].sig2;
           aaf = (float)((double)aaf + sa / dp[d].sig2);
           bbf = (float)((double)bbf + sb / dp[d].sig2);
      }
-     out[p].aa = aa;
-     out[p].bb = bb;
-     out[p].aaf = aaf;
-     out[p].bbf = bbf;
+     if (threadIdx.x == 0) {
+          out[p].aa = aa;
+          out[p].bb = bb;
+          out[p].aaf = aaf;
+          out[p].bbf = bbf;
+     }
 }
 
 // Forward sweep of the natural spline (auxi.c:102-111), u[i] for i in [1, n-2]

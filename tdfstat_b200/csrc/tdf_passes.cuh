@@ -58,16 +58,11 @@ __global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_rowpass(Src sr
      const int c = tid % LINES, t = tid / LINES;
      // first-pass inputs straight from the rows into registers: per load
      // instruction a warp reads 4 consecutive elements of each of 8 rows
-     // (whole 32-byte sectors)
      cx<T> v[NA][8];
      cx<T> *s[NA];
+     src.template load<L>(v, b, k1b + c, t);
 #pragma unroll
-     for (int a = 0; a < NA; a++) {
-          const cx<T> *r = src.row(a, b, k1b + c);
-          s[a] = lines + (a * LINES + c) * G::STRIDE;
-#pragma unroll
-          for (int m = 0; m < 8; m++) v[a][m] = r[t + m * (L / 8)];
-     }
+     for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
      load_table<T>(tw, twline, L);
      __syncthreads();
      line_fft<T, L, SIGN, NA>(v, s, tw, t);
@@ -77,7 +72,9 @@ __global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_rowpass(Src sr
 // ------------------------------------------------------------------ policies
 
 // Column-pass epilogue: multiply by W_N^(n2*k1) and store Y[k1*N2 + n2].
-// Batch b, array a lives at y + ((size_t)b*NA + a)*N.
+// Batch b's arrays are interleaved element by element: array a of element e
+// lives at y[((size_t)b*N + e)*NA + a], so both arrays of a sample move in one
+// access (16 bytes for two float2).
 template <typename T, int SIGN, int NA>
 struct StoreFourstep {
      cx<T> *y;
@@ -87,26 +84,43 @@ struct StoreFourstep {
      template <int L>
      __device__ __forceinline__ void store(const cx<T> (&v)[NA][8], int b, int n2, int t) const {
 #pragma unroll
-          for (int a = 0; a < NA; a++) {
-               cx<T> *dst = y + ((size_t)b * NA + a) * N + n2;
+          for (int m = 0; m < 8; m++) {
+               const int k1 = t + m * (L / 8);
+               const cx<T> w = twsign<SIGN>(fourstep_twiddle<T>(hi, lo, n2 * k1));   // shared by the arrays
+               cx<T> *dst = y + ((size_t)b * N + n2 + (size_t)k1 * N2) * NA;
+               if constexpr (NA == 2 && sizeof(T) == 4) {
+                    const cx<T> p = cmul(v[0][m], w), q = cmul(v[1][m], w);
+                    *reinterpret_cast<float4 *>(dst) = make_float4(p.x, p.y, q.x, q.y);
+               } else {
 #pragma unroll
-               for (int m = 0; m < 8; m++) {
-                    int k1 = t + m * (L / 8);
-                    cx<T> w = twsign<SIGN>(fourstep_twiddle<T>(hi, lo, n2 * k1));
-                    dst[(size_t)k1 * N2] = cmul(v[a][m], w);
+                    for (int a = 0; a < NA; a++) dst[a] = cmul(v[a][m], w);
                }
           }
      }
 };
 
-// Row-pass source: rows of Y laid out as in StoreFourstep.
+// Row-pass source: rows of Y laid out as in StoreFourstep.  load() fills the
+// first-pass inputs v[a][m] = row k1 element t + m*L/8 of every array.
 template <typename T, int NA>
 struct RowsY {
      const cx<T> *y;
      int N;          // N1*N2
      int rowstride;  // N2
-     __device__ __forceinline__ const cx<T> *row(int a, int b, int k1) const {
-          return y + ((size_t)b * NA + a) * N + (size_t)k1 * rowstride;
+     template <int L>
+     __device__ __forceinline__ void load(cx<T> (&v)[NA][8], int b, int k1, int t) const {
+          const cx<T> *r = y + ((size_t)b * N + (size_t)k1 * rowstride) * NA;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               const cx<T> *e = r + (size_t)(t + m * (L / 8)) * NA;
+               if constexpr (NA == 2 && sizeof(T) == 4) {
+                    const float4 q = *reinterpret_cast<const float4 *>(e);
+                    v[0][m] = make_float2(q.x, q.y);
+                    v[1][m] = make_float2(q.z, q.w);
+               } else {
+#pragma unroll
+                    for (int a = 0; a < NA; a++) v[a][m] = e[a];
+               }
+          }
      }
 };
 

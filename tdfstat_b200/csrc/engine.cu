@@ -19,6 +19,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "tdfcuda.h"
 #include "tdf_kernels.cuh"
 
@@ -59,18 +61,39 @@ static int set_error(int code, const char *fmt, ...) {
 static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 static int ilog2i(int n) { int l = 0; while ((1 << l) < n) l++; return l; }
 
+// kernel attributes already set, per (kernel, device): the largest dynamic
+// shared memory asked for so far
+static std::mutex g_attr_mu;
+static std::vector<std::pair<std::pair<const void *, int>, size_t>> g_attr;
+
 template <class K>
 static int set_smem(K kern, size_t smem) {
+     int dev = 0;
+     CUCHK(cudaGetDevice(&dev));
+     const std::pair<const void *, int> key((const void *)kern, dev);
+     {
+          std::lock_guard<std::mutex> lk(g_attr_mu);
+          for (const auto &a : g_attr)
+               if (a.first == key && a.second >= smem) return TDF_OK;
+     }
      if (smem > 48 * 1024) CUCHK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
      // the FFT passes live in shared memory: ask for the largest carveout so
      // that more than one CTA fits per SM
      CUCHK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+     std::lock_guard<std::mutex> lk(g_attr_mu);
+     for (auto &a : g_attr)
+          if (a.first == key) {
+               a.second = std::max(a.second, smem);
+               return TDF_OK;
+          }
+     g_attr.push_back({key, smem});
      return TDF_OK;
 }
 
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
 static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
-     constexpr size_t smem = pass_smem_bytes<T, L, NA>();
+     size_t smem = pass_smem_bytes<T, L, NA>();
+     if constexpr (is_staged<Pro>::value) smem = pro.smem;
      auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi>;
      TRY(set_smem(kern, smem));
      kern<<<grid, L, smem, st>>>(pro, epi, tw);
@@ -233,8 +256,26 @@ struct tdf_engine {
      DevBuf skyp[2], B0, B1, B2, shftf, partial, aabb[2];
      // operands
      DevBuf xab[2], s2[2], xa64[2], xb64[2], t1[2];   // per batch slot
-     // spindown stage
-     DevBuf tparam, Ybuf, Fbuf, mubuf, tcnt, linesd, cand;
+     // TMA staging of the split-form operands in the column pass
+     bool staged = false;
+     CUtensorMap tm_x[2], tm_s[2];   // xab[k], s2[k]
+     int stg_groups = 0, stg_stages = 0;
+     unsigned stg_bar_off = 0, stg_smem = 0;
+     // spindown stage: consecutive resolve groups alternate between lanes,
+     // each with its own stream and buffers, so that one lane's kernel tails
+     // and trigger resolution overlap the other lane's passes
+     struct Lane {
+          DevBuf Ybuf;    // four-step intermediate of a chunk
+          DevBuf Fbuf;    // F ring of a resolve group
+          DevBuf mubuf;   // blocks_avg means of a resolve group
+          DevBuf tcnt;    // per-template trigger counts + candidate count
+          DevBuf cand;    // candidate bins of a resolve group
+     };
+     Lane ln[2];
+     int nlanes = 2;                       // TDF_LANES=1 runs every group on the engine stream
+     cudaStream_t lane_own = nullptr;      // stream of lane 1 (lane 0 runs on `stream`)
+     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+     DevBuf tparam, linesd;
      unsigned cand_cap = 0;
      // two batch slots: while the host drains one slot's triggers the
      // device runs the other slot's batch
@@ -359,6 +400,88 @@ static int upload_inputs(tdf_engine *e, const tdf_segment *s) {
      return TDF_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda); null when the driver does not provide it
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+     static std::once_flag once;
+     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+     std::call_once(once, [] {
+          void *p = nullptr;
+          cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+          if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+              q == cudaDriverEntryPointSuccess)
+               fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+     });
+     return fn;
+}
+
+template <int L>
+static void col_geometry(size_t *smem, int *blocks) {
+     *smem = pass_smem_bytes<float, L, 2>();
+     *blocks = pass_min_blocks<float, L>();
+}
+
+// Sizes the TMA ring of the split-form column pass (DemodSplitStaged) and
+// encodes the operand tensor maps of both batch slots.  The ring takes as
+// many row groups as fit in the shared memory a CTA may use at the pass's
+// occupancy (228 KB per SM, 1 KB reserved per CTA).  Used with
+// TDF_STAGED_OPERANDS=1; by default the column pass loads its operands per
+// thread (DemodSplit), which measured as fast with the operands L2-resident.
+static int staged_setup(tdf_engine *e) {
+     e->staged = false;
+     if (e->form != TDF_FORM_SPLIT) return TDF_OK;
+     const char *env = getenv("TDF_STAGED_OPERANDS");
+     if (!env || env[0] != '1') return TDF_OK;
+     const int L = e->t_f32.N1, N2 = e->t_f32.N2, R = L / 8, nifo = e->nifo;
+     if (e->Nal % N2 != 0) return TDF_OK;
+     size_t pass_smem = 0;
+     int blocks = 1;
+     switch (L) {
+     case 64: col_geometry<64>(&pass_smem, &blocks); break;
+     case 128: col_geometry<128>(&pass_smem, &blocks); break;
+     case 256: col_geometry<256>(&pass_smem, &blocks); break;
+     case 512: col_geometry<512>(&pass_smem, &blocks); break;
+     case 1024: col_geometry<1024>(&pass_smem, &blocks); break;
+     default: return TDF_OK;
+     }
+     const size_t tw = (size_t)L * sizeof(float2);
+     const size_t lines = pass_smem - tw;
+     const size_t slot = (size_t)nifo * R * LINES * (sizeof(float4) + sizeof(float));
+     const size_t bars = 8 * sizeof(uint64_t);
+     const int rows = (e->N + N2 - 1) / N2;
+     const int groups = std::min(8, (rows + R - 1) / R);
+     const size_t budget = std::min<size_t>(227 * 1024, 233472 / blocks - 1024);
+     if (budget < tw + bars + slot) return TDF_OK;
+     const int stages = (int)std::min<size_t>((size_t)groups, (budget - tw - bars) / slot);
+     const size_t area = std::max(lines, (size_t)stages * slot);
+     PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+     if (!encode) return TDF_OK;
+     for (int k = 0; k < 2; k++) {
+          const cuuint64_t rowsx = (cuuint64_t)(e->Nal / N2);
+          const cuuint64_t dx[4] = {(cuuint64_t)4 * N2, rowsx, (cuuint64_t)nifo, (cuuint64_t)e->Bs};
+          const cuuint64_t sx[3] = {(cuuint64_t)N2 * 16, (cuuint64_t)e->Nal * 16, (cuuint64_t)nifo * e->Nal * 16};
+          const cuuint32_t bx[4] = {4 * LINES, (cuuint32_t)R, (cuuint32_t)nifo, 1};
+          const cuuint64_t ds[4] = {(cuuint64_t)N2, rowsx, (cuuint64_t)nifo, (cuuint64_t)e->Bs};
+          const cuuint64_t ss[3] = {(cuuint64_t)N2 * 4, (cuuint64_t)e->Nal * 4, (cuuint64_t)nifo * e->Nal * 4};
+          const cuuint32_t bs[4] = {LINES, (cuuint32_t)R, (cuuint32_t)nifo, 1};
+          const cuuint32_t one[4] = {1, 1, 1, 1};
+          CUresult r = encode(&e->tm_x[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, e->xab[k].p, dx, sx, bx, one,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+          if (r != CUDA_SUCCESS) return set_error(TDF_ERR_CUDA, "cuTensorMapEncodeTiled (operands xab): %d", (int)r);
+          r = encode(&e->tm_s[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, e->s2[k].p, ds, ss, bs, one,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+          if (r != CUDA_SUCCESS) return set_error(TDF_ERR_CUDA, "cuTensorMapEncodeTiled (operands s2): %d", (int)r);
+     }
+     e->stg_groups = groups;
+     e->stg_stages = stages;
+     e->stg_bar_off = (unsigned)(tw + area);
+     e->stg_smem = (unsigned)(tw + area + bars);
+     e->staged = true;
+     return TDF_OK;
+}
+
 static int engine_alloc(tdf_engine *e) {
      const int nifo = e->nifo, Bs = e->Bs, Tc = e->TcMax;
      const size_t Q = (size_t)Bs * nifo;
@@ -404,13 +527,17 @@ static int engine_alloc(tdf_engine *e) {
      }
      const size_t csz = e->form == TDF_FORM_SPLIT ? sizeof(float2) : sizeof(double2);
      const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
-     TRY(e->Ybuf.alloc((size_t)Tc * 2 * e->nfftf * csz));
      const size_t G = (size_t)kGroup * Tc;   // templates per resolve group
-     TRY(e->Fbuf.alloc(G * e->nF * rsz));
-     TRY(e->mubuf.alloc(G * std::max(1, e->nblk_mu) * rsz));
-     TRY(e->tcnt.alloc((G + 1) * sizeof(unsigned)));
      e->cand_cap = (unsigned)G * 4096u;
-     TRY(e->cand.alloc(e->cand_cap * sizeof(uint2)));
+     for (int l = 0; l < e->nlanes; l++) {
+          tdf_engine::Lane &L = e->ln[l];
+          TRY(L.Ybuf.alloc((size_t)Tc * 2 * e->nfftf * csz));
+          TRY(L.Fbuf.alloc(G * e->nF * rsz));
+          TRY(L.mubuf.alloc(G * std::max(1, e->nblk_mu) * rsz));
+          TRY(L.tcnt.alloc((G + 1) * sizeof(unsigned)));
+          CUCHK(cudaMemset(L.tcnt.p, 0, L.tcnt.bytes));
+          TRY(L.cand.alloc(e->cand_cap * sizeof(uint2)));
+     }
      TRY(e->linesd.alloc(std::max<size_t>(1, e->lines.size()) * sizeof(double)));
      if (!e->lines.empty())
           CUCHK(cudaMemcpy(e->linesd.p, e->lines.data(), e->lines.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -427,6 +554,7 @@ static int engine_alloc(tdf_engine *e) {
      TRY(e->t_ninterp.build(e->Ninterp));
      if (e->form == TDF_FORM_SPLIT) TRY(e->t_f32.build(e->nfftf));
      else TRY(e->t_f64.build(e->nfftf));
+     TRY(staged_setup(e));
      return TDF_OK;
 }
 
@@ -434,9 +562,16 @@ static void engine_free(tdf_engine *e) {
      DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp[0],
                        &e->skyp[1], &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb[0], &e->aabb[1],
                        &e->xab[0], &e->xab[1], &e->s2[0], &e->s2[1], &e->xa64[0], &e->xa64[1], &e->xb64[0],
-                       &e->xb64[1], &e->t1[0], &e->t1[1], &e->tparam, &e->Ybuf, &e->Fbuf, &e->mubuf,
-                       &e->trig[0], &e->trig[1], &e->counters[0], &e->counters[1], &e->tcnt, &e->linesd, &e->cand};
+                       &e->xb64[1], &e->t1[0], &e->t1[1], &e->tparam, &e->trig[0], &e->trig[1],
+                       &e->counters[0], &e->counters[1], &e->linesd};
      for (DevBuf *b : bufs) b->release();
+     for (tdf_engine::Lane &L : e->ln) {
+          L.Ybuf.release();
+          L.Fbuf.release();
+          L.mubuf.release();
+          L.tcnt.release();
+          L.cand.release();
+     }
      e->t_nfft.release();
      e->t_ninterp.release();
      e->t_f32.release();
@@ -460,6 +595,11 @@ static void engine_free(tdf_engine *e) {
           if (e->spin_done[k]) cudaEventDestroy(e->spin_done[k]);
           e->sky_done[k] = e->spin_done[k] = nullptr;
      }
+     if (e->fork_ev) cudaEventDestroy(e->fork_ev);
+     if (e->join_ev) cudaEventDestroy(e->join_ev);
+     e->fork_ev = e->join_ev = nullptr;
+     if (e->lane_own) cudaStreamDestroy(e->lane_own);
+     e->lane_own = nullptr;
      if (e->sky_stream) cudaStreamDestroy(e->sky_stream);
      e->sky_stream = nullptr;
      if (e->own) cudaStreamDestroy(e->own);
@@ -605,9 +745,12 @@ static int run_sky_stage(tdf_engine *e, int npts) {
 // Spindown stage, FFT part, for chunk `ci` of a resolve group whose templates
 // start at dtp: the column pass (demodulation + first FFT pass) and the row
 // pass (second FFT pass + F + candidate bins) for nt templates.
+static cudaStream_t lane_stream(const tdf_engine *e, int l) { return l == 0 ? e->stream : e->lane_own; }
+
 template <typename T>
-static int run_chunk(tdf_engine *e, const TmplParam *dtp, int ci, int nt) {
-     cudaStream_t st = e->stream;
+static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt) {
+     cudaStream_t st = lane_stream(e, l);
+     tdf_engine::Lane &Ln = e->ln[l];
      const FFTTables<T> *tb;
      if constexpr (std::is_same<T, float>::value) tb = &e->t_f32;
      else tb = &e->t_f64;
@@ -615,26 +758,42 @@ static int run_chunk(tdf_engine *e, const TmplParam *dtp, int ci, int nt) {
      const int boff = ci * e->Tc;
      const TmplParam *ctp = dtp + boff;
      const unsigned G = (unsigned)kGroup * e->Tc;
-     unsigned *tcnt = e->tcnt.as<unsigned>();
-     StoreFourstep<T, -1, 2> epi{e->Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
-     size_t tev = e->timing ? timing_begin(e) : (size_t)-1;
+     unsigned *tcnt = Ln.tcnt.as<unsigned>();
+     StoreFourstep<T, -1, 2> epi{Ln.Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
+     size_t tev = e->timing ? timing_begin(e, st) : (size_t)-1;
      if constexpr (std::is_same<T, float>::value) {
-          DemodSplit pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal, e->nifo};
-          TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
+          if (e->staged) {
+               DemodSplitStaged pro;
+               pro.mx = e->tm_x[e->cur];
+               pro.ms = e->tm_s[e->cur];
+               pro.tp = ctp;
+               pro.err = reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1);
+               pro.N = e->N;
+               pro.N2 = t.N2;
+               pro.nifo = e->nifo;
+               pro.groups = e->stg_groups;
+               pro.stages = e->stg_stages;
+               pro.bar_off = e->stg_bar_off;
+               pro.smem = e->stg_smem;
+               TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
+          } else {
+               DemodSplit pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal, e->nifo};
+               TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
+          }
      } else {
           DemodFP64 pro{e->xa64[e->cur].as<double2>(), e->xb64[e->cur].as<double2>(), e->t1[e->cur].as<double>(), ctp,
                         e->N, t.N2, e->Nal, e->nifo};
           TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
      }
-     if (e->timing) timing_end(e, tev, KT_COL, nt);
+     if (e->timing) timing_end(e, tev, KT_COL, nt, st);
      const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
-     RowsY<T, 2> src{e->Ybuf.as<cx<T>>(), e->nfftf, t.N2};
-     StoreFstat<T> epi2{e->Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF, e->opts.fr[0],
-                        e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : e->cand.as<uint2>(), tcnt + G,
+     RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
+     StoreFstat<T> epi2{Ln.Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF, e->opts.fr[0],
+                        e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G,
                         e->cand_cap, boff};
-     tev = e->timing ? timing_begin(e) : (size_t)-1;
+     tev = e->timing ? timing_begin(e, st) : (size_t)-1;
      TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
-     if (e->timing) timing_end(e, tev, KT_ROW, nt);
+     if (e->timing) timing_end(e, tev, KT_ROW, nt, st);
      e->launches += 2;
      return TDF_OK;
 }
@@ -643,11 +802,12 @@ static int run_chunk(tdf_engine *e, const TmplParam *dtp, int ci, int nt) {
 // dtp; their F spectra fill the F ring in order): the candidate bins the row
 // passes collected, or, with blocks_avg, block means and a scan of every bin.
 template <typename T>
-static int run_resolve(tdf_engine *e, const TmplParam *dtp, int ntg) {
-     cudaStream_t st = e->stream;
+static int run_resolve(tdf_engine *e, int l, const TmplParam *dtp, int ntg) {
+     cudaStream_t st = lane_stream(e, l);
+     tdf_engine::Lane &Ln = e->ln[l];
      const bool split = std::is_same<T, float>::value;
      const unsigned G = (unsigned)kGroup * e->Tc;
-     unsigned *tcnt = e->tcnt.as<unsigned>();
+     unsigned *tcnt = Ln.tcnt.as<unsigned>();
      const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
      unsigned long long *cnt = e->counters[e->cur].as<unsigned long long>();
      ThrArgs A;
@@ -666,38 +826,53 @@ static int run_resolve(tdf_engine *e, const TmplParam *dtp, int ntg) {
      A.cnt = cnt;
      A.tcnt = tcnt;
      A.err = reinterpret_cast<unsigned *>(cnt + 1);
-     size_t tev = e->timing ? timing_begin(e) : (size_t)-1;
+     size_t tev = e->timing ? timing_begin(e, st) : (size_t)-1;
      if (blocks) {
-          k_block_means<T><<<dim3(e->nblk_mu, ntg), 256, 0, st>>>(e->Fbuf.as<T>(), e->nF, e->nblk_mu, e->mubuf.as<T>());
+          k_block_means<T><<<dim3(e->nblk_mu, ntg), 256, 0, st>>>(Ln.Fbuf.as<T>(), e->nF, e->nblk_mu, Ln.mubuf.as<T>());
           CUCHK(cudaGetLastError());
           dim3 g((e->nF + 255) / 256, ntg);
-          if (split) k_threshold<T, false><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->mubuf.as<T>(), A);
-          else k_threshold<T, true><<<g, 256, 0, st>>>(e->Fbuf.as<T>(), e->mubuf.as<T>(), A);
+          if (split) k_threshold<T, false><<<g, 256, 0, st>>>(Ln.Fbuf.as<T>(), Ln.mubuf.as<T>(), A);
+          else k_threshold<T, true><<<g, 256, 0, st>>>(Ln.Fbuf.as<T>(), Ln.mubuf.as<T>(), A);
           e->launches += 2;
      } else {
-          if (split) k_resolve<T, false><<<64, 256, 0, st>>>(e->Fbuf.as<T>(), A, e->cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
-          else k_resolve<T, true><<<64, 256, 0, st>>>(e->Fbuf.as<T>(), A, e->cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
+          if (split) k_resolve<T, false><<<64, 256, 0, st>>>(Ln.Fbuf.as<T>(), A, Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
+          else k_resolve<T, true><<<64, 256, 0, st>>>(Ln.Fbuf.as<T>(), A, Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
           e->launches++;
      }
      CUCHK(cudaGetLastError());
-     if (e->timing) timing_end(e, tev, KT_THR, ntg);
+     if (e->timing) timing_end(e, tev, KT_THR, ntg, st);
      // ready for the next group: trigger counters and candidate count
      CUCHK(cudaMemsetAsync(tcnt, 0, (G + 1) * sizeof(unsigned), st));
      return TDF_OK;
 }
 
-// the spindown stage of nt templates starting at dtp: groups of chunks
+// The spindown stage of nt templates starting at dtp: resolve groups of
+// chunks, group k on lane k % nlanes.  Lane 1 starts after everything queued
+// on the engine stream so far (sky stage, template upload) and the engine
+// stream waits for it at the end, so callers see one ordered stream.
 static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
      const int G = kGroup * e->Tc;
-     for (int g0 = 0; g0 < nt; g0 += G) {
+     const int ngroups = (nt + G - 1) / G;
+     const int lanes = std::min(e->nlanes, ngroups);
+     if (lanes > 1) {
+          CUCHK(cudaEventRecord(e->fork_ev, e->stream));
+          CUCHK(cudaStreamWaitEvent(e->lane_own, e->fork_ev, 0));
+     }
+     for (int gi = 0; gi < ngroups; gi++) {
+          const int g0 = gi * G;
+          const int l = gi % lanes;
           const int ntg = std::min(G, nt - g0);
           for (int ci = 0; ci * e->Tc < ntg; ci++) {
                const int n = std::min(e->Tc, ntg - ci * e->Tc);
-               if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, dtp + g0, ci, n));
-               else TRY(run_chunk<double>(e, dtp + g0, ci, n));
+               if (e->form == TDF_FORM_SPLIT) TRY(run_chunk<float>(e, l, dtp + g0, ci, n));
+               else TRY(run_chunk<double>(e, l, dtp + g0, ci, n));
           }
-          if (e->form == TDF_FORM_SPLIT) TRY(run_resolve<float>(e, dtp + g0, ntg));
-          else TRY(run_resolve<double>(e, dtp + g0, ntg));
+          if (e->form == TDF_FORM_SPLIT) TRY(run_resolve<float>(e, l, dtp + g0, ntg));
+          else TRY(run_resolve<double>(e, l, dtp + g0, ntg));
+     }
+     if (lanes > 1) {
+          CUCHK(cudaEventRecord(e->join_ev, e->lane_own));
+          CUCHK(cudaStreamWaitEvent(e->stream, e->join_ev, 0));
      }
      return TDF_OK;
 }
@@ -726,6 +901,8 @@ static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_tot
      const unsigned errf = (unsigned)(e->h_cnt[2 * slot + 1] & 0xffffffffu);
      if (errf & ERR_OVERFLOW)
           return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
+     if (errf & ERR_STAGE_TIMEOUT)
+          return set_error(TDF_ERR_CUDA, "column pass: an operand copy did not complete within the wait limit");
      if (nfound > e->trig_cap) {
           *over = true;
           e->h_cnt[2 * slot] = nfound;   // keep the needed size visible
@@ -780,7 +957,7 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
           CUCHK(cudaStreamSynchronize(e->sky_stream));
           CUCHK(cudaStreamSynchronize(e->stream));
           for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
-          CUCHK(cudaMemsetAsync(e->tcnt.p, 0, e->tcnt.bytes, e->stream));
+          for (int l = 0; l < e->nlanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
           int pending[2] = {0, 0};
           bool over = false;
           size_t b = 0;
@@ -960,7 +1137,9 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      e->nfftf = seg->nfftf;
      e->Ninterp = seg->Ninterp;
      e->nifo = seg->nifo;
-     e->Nal = (seg->N + 255) / 256 * 256;
+     // a multiple of every row length N2 <= 1024 of the four-step split, so
+     // that the operand arrays view as whole rows for the TMA boxes
+     e->Nal = (seg->N + 1023) / 1024 * 1024;
      e->n2N = seg->interpftpad * seg->N;
      e->nF = opts->fr[1] - opts->fr[0] + 1;
      e->nblk_mu = opts->blocks_avg ? (opts->fr[1] - opts->fr[0]) / TDF_NAVFSTAT : 0;
@@ -970,6 +1149,8 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      e->TcMax = std::max(48, e->Tc);
      const char *ov = getenv("TDF_SKY_OVERLAP");
      e->overlap = ov && atoi(ov) != 0;   // measured: off is faster when the spindown kernels fill the GPU
+     const char *nl = getenv("TDF_LANES");
+     if (nl && atoi(nl) == 1) e->nlanes = 1;
      autotune_cache_lookup(e);
      e->lines.assign(opts->lines, opts->lines + 2 * (size_t)opts->numlines);
      e->opts.lines = nullptr;
@@ -977,6 +1158,9 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      int st = TDF_OK;
      cudaError_t ce = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking);
      if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->sky_stream, cudaStreamNonBlocking);
+     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->lane_own, cudaStreamNonBlocking);
+     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
+     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join_ev, cudaEventDisableTiming);
      for (int k = 0; k < 2 && ce == cudaSuccess; k++) {
           ce = cudaEventCreateWithFlags(&e->sky_done[k], cudaEventDisableTiming);
           if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->spin_done[k], cudaEventDisableTiming);
@@ -1017,6 +1201,7 @@ int tdf_engine_destroy(tdf_engine *e) {
      if (!e) return TDF_OK;
      cudaSetDevice(e->dev);
      if (e->sky_stream) cudaStreamSynchronize(e->sky_stream);
+     if (e->lane_own) cudaStreamSynchronize(e->lane_own);
      if (e->stream) cudaStreamSynchronize(e->stream);
      engine_free(e);
      delete e;
@@ -1152,21 +1337,25 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[0], 0));
      CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[0], sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
      CUCHK(cudaMemsetAsync(e->counters[0].p, 0, 2 * sizeof(unsigned long long), e->stream));
-     CUCHK(cudaMemsetAsync(e->tcnt.p, 0, e->tcnt.bytes, e->stream));
+     for (int l = 0; l < e->nlanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
      TRY(run_templates(e, e->tparam.as<TmplParam>(), 1));
+     CUCHK(cudaMemcpyAsync(e->h_cnt, e->counters[0].p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     if (e->h_cnt[1] & ERR_STAGE_TIMEOUT)
+          return set_error(TDF_ERR_CUDA, "column pass: an operand copy did not complete within the wait limit");
      const int n = e->nF;
      if (e->form == TDF_FORM_SPLIT) {
           std::vector<float> f(n), mu(std::max(1, e->nblk_mu));
-          CUCHK(cudaMemcpyAsync(f.data(), e->Fbuf.p, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+          CUCHK(cudaMemcpyAsync(f.data(), e->ln[0].Fbuf.p, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
           if (e->nblk_mu)
-               CUCHK(cudaMemcpyAsync(mu.data(), e->mubuf.p, e->nblk_mu * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+               CUCHK(cudaMemcpyAsync(mu.data(), e->ln[0].mubuf.p, e->nblk_mu * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
           CUCHK(cudaStreamSynchronize(e->stream));
           for (int i = 0; i < n; i++) F[i] = (i < e->nblk_mu * TDF_NAVFSTAT) ? (double)(f[i] / mu[i >> 12]) : (double)f[i];
      } else {
           std::vector<double> mu(std::max(1, e->nblk_mu));
-          CUCHK(cudaMemcpyAsync(F, e->Fbuf.p, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+          CUCHK(cudaMemcpyAsync(F, e->ln[0].Fbuf.p, n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
           if (e->nblk_mu)
-               CUCHK(cudaMemcpyAsync(mu.data(), e->mubuf.p, e->nblk_mu * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+               CUCHK(cudaMemcpyAsync(mu.data(), e->ln[0].mubuf.p, e->nblk_mu * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
           CUCHK(cudaStreamSynchronize(e->stream));
           for (int i = 0; i < n && i < e->nblk_mu * TDF_NAVFSTAT; i++) F[i] = F[i] / mu[i >> 12];
      }

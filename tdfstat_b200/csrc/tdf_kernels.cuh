@@ -13,6 +13,7 @@
 //                     division by sig2, conversion to the spindown operands
 //   spindown stage (once per template)
 //     DemodSplit /
+//     DemodSplitStaged /
 //     DemodFP64       column-pass prologues: spindown_modulation
 //                     (spinmod.c:490-514) fused into the first FFT pass
 //     StoreFstat      row-pass epilogue: F = |Fa|^2/aa + |Fb|^2/bb
@@ -23,6 +24,7 @@
 #pragma once
 
 #include <float.h>
+#include "tdf_bulk.cuh"
 #include "tdf_passes.cuh"
 
 namespace tdf {
@@ -57,6 +59,7 @@ struct Trig {
 };
 
 constexpr unsigned ERR_OVERFLOW = 1u;
+constexpr unsigned ERR_STAGE_TIMEOUT = 2u;   // an operand copy did not complete within the wait limit
 constexpr double TWO_PI = 6.283185307179586476925286766559;
 constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
 constexpr double M_PI_D = 3.14159265358979323846;
@@ -382,6 +385,109 @@ struct DemodSplit {
                     v[1][kQ * h + q] = fb[q];
                }
           }
+     }
+};
+
+// DemodSplit with its operands brought in by TMA.  Thread (c, t) of the CTA
+// needs, for element m, the samples of row n1 = t + m*R (R = L/8) of column
+// n2 = x0 + c, so the rows of a group m of the CTA's LINES columns, every
+// detector, form one box of each operand tensor:
+//   xab as floats {4*N2, rows, nifo, slots}, box {4*LINES, R, nifo, 1}
+//   s2            {N2,   rows, nifo, slots}, box {LINES,   R, nifo, 1}
+// (rows = Nal/N2, Nal a multiple of N2).  The groups holding samples < N go
+// through a ring of `stages` shared-memory slots that aliases the line
+// buffers (unused until the first FFT pass stores), each slot completing on
+// its own mbarrier; all copies of the ring are in flight while the threads
+// demodulate, instead of one element's loads per thread at a time.
+// The arithmetic per element is DemodSplit's, in the same order.
+struct DemodSplitStaged {
+     CUtensorMap mx;    // xab
+     CUtensorMap ms;    // s2
+     const TmplParam *tp;
+     unsigned *err;     // ERR_STAGE_TIMEOUT is or-ed in when a wait gives up
+     int N, N2, nifo;
+     int groups;        // row groups holding samples < N (<= 8)
+     int stages;        // ring slots (>= 1)
+     unsigned bar_off;  // byte offset of the ring's mbarriers in dynamic shared memory
+     unsigned smem;     // dynamic shared memory of the launch
+     static constexpr bool kStaged = true;
+
+     template <int L>
+     __device__ __forceinline__ void issue(int g, int s, unsigned char *ring, uint64_t *bars, unsigned slot_bytes,
+                                           unsigned xbytes, int x0, int w) const {
+          unsigned char *dst = ring + (size_t)s * slot_bytes;
+          mbar_expect_tx(&bars[s], slot_bytes);
+          tma_load_4d(dst, &mx, 4 * x0, g * (L / 8), 0, w, &bars[s]);
+          tma_load_4d(dst + xbytes, &ms, x0, g * (L / 8), 0, w, &bars[s]);
+     }
+
+     template <int L>
+     __device__ __forceinline__ void load_staged(float2 (&v)[2][8], int b, int n2, int t, unsigned char *ring,
+                                                 uint64_t *bars) const {
+          constexpr int R = L / 8;
+          const TmplParam P = tp[b];
+          const float spf = (float)P.spnd;
+          const unsigned xbytes = (unsigned)nifo * R * LINES * 16;
+          const unsigned slot_bytes = xbytes + (unsigned)nifo * R * LINES * 4;
+          const int x0 = blockIdx.x * LINES;
+          const int c = threadIdx.x % LINES;
+          if (threadIdx.x == 0) {
+               for (int s = 0; s < stages; s++) mbar_init(&bars[s], 1);
+               mbar_fence_init();
+          }
+          __syncthreads();
+          if (threadIdx.x == 0)
+               for (int g = 0; g < stages; g++) issue<L>(g, g, ring, bars, slot_bytes, xbytes, x0, (int)P.slot);
+          bool waited = true;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
+               if (m < groups) {
+                    const int s = m % stages;
+                    waited &= mbar_wait(&bars[s], (unsigned)(m / stages) & 1u);
+                    const unsigned char *sl = ring + (size_t)s * slot_bytes;
+                    const float4 *X = reinterpret_cast<const float4 *>(sl);
+                    const float *S2 = reinterpret_cast<const float *>(sl + xbytes);
+                    const int i = N2 * (t + m * R) + n2;
+                    if (i < N) {
+                         const double di = (double)i;
+                         const double ph = fma(P.spnd, di * di, P.het1 * di);
+                         const double kk = rint(ph * INV_TWO_PI);
+                         const float pr = (float)fma(-kk, TWO_PI, ph);
+                         const int e0 = t * LINES + c;
+                         if (nifo <= 2) {
+                              DemodSplit::rot(X[e0], fmaf(spf, S2[e0], pr), fa, fb);
+                              if (nifo == 2) {
+                                   const int e1 = (R + t) * LINES + c;
+                                   float2 pa, pb;
+                                   DemodSplit::rot(X[e1], fmaf(spf, S2[e1], pr), pa, pb);
+                                   fa = cadd(fa, pa);
+                                   fb = cadd(fb, pb);
+                              }
+                         } else {
+                              CompSum ar, ai, br, bi;
+                              for (int d = 0; d < nifo; d++) {
+                                   const int ed = (d * R + t) * LINES + c;
+                                   float2 pa, pb;
+                                   DemodSplit::rot(X[ed], fmaf(spf, S2[ed], pr), pa, pb);
+                                   if (d == 0) { ar.init(pa.x); ai.init(pa.y); br.init(pb.x); bi.init(pb.y); }
+                                   else { ar.add(pa.x); ai.add(pa.y); br.add(pb.x); bi.add(pb.y); }
+                              }
+                              fa = make_float2(ar.value(), ai.value());
+                              fb = make_float2(br.value(), bi.value());
+                         }
+                    }
+                    if (m + stages < groups) {
+                         // every thread is done with slot s: refill it
+                         __syncthreads();
+                         if (threadIdx.x == 0)
+                              issue<L>(m + stages, s, ring, bars, slot_bytes, xbytes, x0, (int)P.slot);
+                    }
+               }
+               v[0][m] = fa;
+               v[1][m] = fb;
+          }
+          if (!waited) atomicOr(err, ERR_STAGE_TIMEOUT);
      }
 };
 

@@ -10,6 +10,8 @@
 //     the rows straight into registers, Epi::store consumes X[k1 + N1*k2].
 #pragma once
 
+#include <type_traits>
+
 #include "tdf_fft.cuh"
 
 namespace tdf {
@@ -25,10 +27,19 @@ constexpr int pass_min_blocks() {
      return sizeof(T) == 4 ? (L <= 256 ? 3 : (L == 512 ? 2 : 1)) : 1;
 }
 
+// A prologue with `static constexpr bool kStaged = true` stages its operands
+// through shared memory itself: load_staged() gets the line-buffer area (free
+// until the first pass stores) and its barriers at byte offset pro.bar_off.
+template <class P, class = void>
+struct is_staged : std::false_type {};
+template <class P>
+struct is_staged<P, std::void_t<decltype(P::kStaged)>> : std::integral_constant<bool, P::kStaged> {};
+
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
-__global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_colpass(Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
+__global__ void __launch_bounds__(L, (pass_min_blocks<T, L>()))
+k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
-     extern __shared__ __align__(16) unsigned char smem_raw[];
+     extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
      load_table<T>(tw, twline, L);
@@ -37,7 +48,11 @@ __global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_colpass(Pro pr
      const int n2 = blockIdx.x * LINES + c;
      const int b = blockIdx.y;
      cx<T> v[NA][8];
-     pro.template load<L>(v, b, n2, t);
+     if constexpr (is_staged<Pro>::value)
+          pro.template load_staged<L>(v, b, n2, t, reinterpret_cast<unsigned char *>(lines),
+                                      reinterpret_cast<uint64_t *>(smem_raw + pro.bar_off));
+     else
+          pro.template load<L>(v, b, n2, t);
      cx<T> *s[NA];
 #pragma unroll
      for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
@@ -49,7 +64,7 @@ __global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_colpass(Pro pr
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
 __global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
-     extern __shared__ __align__(16) unsigned char smem_raw[];
+     extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
      const int tid = threadIdx.x;

@@ -212,8 +212,6 @@ struct FFTTables {
      const cx<T> *o() const { return lo.as<cx<T>>(); }
 };
 
-// chunks whose F spectra share one trigger-selection launch
-constexpr int kGroup = 4;
 
 // host view of one template
 struct HostTmpl {
@@ -247,6 +245,7 @@ struct tdf_engine {
      int Bs = 8;        // sky points per batch
      int Tc = 16;       // templates per chunk (intermediate spectra sized for L2)
      int TcMax = 32;    // buffers are sized for chunks up to this size
+     int Gt = 64;       // templates per resolve group at most (whole chunks; TDF_GROUP_TEMPLATES)
      int64_t launches = 0;
      FFTTables<double> t_nfft, t_ninterp, t_f64;
      FFTTables<float> t_f32;
@@ -271,10 +270,11 @@ struct tdf_engine {
           DevBuf tcnt;    // per-template trigger counts + candidate count
           DevBuf cand;    // candidate bins of a resolve group
      };
-     Lane ln[2];
-     int nlanes = 2;                       // TDF_LANES=1 runs every group on the engine stream
-     cudaStream_t lane_own = nullptr;      // stream of lane 1 (lane 0 runs on `stream`)
-     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+     static constexpr int kMaxLanes = 4;
+     Lane ln[kMaxLanes];
+     int nlanes = 3;                                  // TDF_LANES=n (1..4)
+     cudaStream_t lane_own[kMaxLanes] = {};          // streams of lanes 1.. (lane 0 runs on `stream`)
+     cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes] = {};
      DevBuf tparam, linesd;
      unsigned cand_cap = 0;
      // two batch slots: while the host drains one slot's triggers the
@@ -293,6 +293,28 @@ struct tdf_engine {
      std::vector<tdf_record> last_recs;
      std::vector<float> last_pairs;
      std::vector<int32_t> last_per;
+     // CUDA graphs of the spindown stage of a batch, keyed by everything the
+     // captured launches bake in; captured on the second sighting of a key
+     struct GraphKey {
+          int slot, nt, Tc, Gt, lanes;
+          const void *tp, *trig;
+          unsigned long long trig_cap;
+          bool operator==(const GraphKey &o) const {
+               return slot == o.slot && nt == o.nt && Tc == o.Tc && Gt == o.Gt && lanes == o.lanes && tp == o.tp &&
+                      trig == o.trig && trig_cap == o.trig_cap;
+          }
+     };
+     struct GraphEntry {
+          GraphKey key;
+          int seen = 0;
+          cudaGraphExec_t exec = nullptr;
+          int64_t launches = 0;   // kernels per replay
+          uint64_t last = 0;
+     };
+     static constexpr size_t kMaxGraphs = 8;
+     std::vector<GraphEntry> graphs;
+     uint64_t graph_tick = 0;
+     bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
      // optional per-kernel event timing
      bool timing = false;
      tdf_kernel_times kt{};
@@ -527,7 +549,7 @@ static int engine_alloc(tdf_engine *e) {
      }
      const size_t csz = e->form == TDF_FORM_SPLIT ? sizeof(float2) : sizeof(double2);
      const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
-     const size_t G = (size_t)kGroup * Tc;   // templates per resolve group
+     const size_t G = (size_t)std::max(e->Gt, Tc);   // templates per resolve group at most
      e->cand_cap = (unsigned)G * 4096u;
      for (int l = 0; l < e->nlanes; l++) {
           tdf_engine::Lane &L = e->ln[l];
@@ -558,7 +580,14 @@ static int engine_alloc(tdf_engine *e) {
      return TDF_OK;
 }
 
+static void graphs_clear(tdf_engine *e) {
+     for (auto &g : e->graphs)
+          if (g.exec) cudaGraphExecDestroy(g.exec);
+     e->graphs.clear();
+}
+
 static void engine_free(tdf_engine *e) {
+     graphs_clear(e);
      DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp[0],
                        &e->skyp[1], &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb[0], &e->aabb[1],
                        &e->xab[0], &e->xab[1], &e->s2[0], &e->s2[1], &e->xa64[0], &e->xa64[1], &e->xb64[0],
@@ -596,10 +625,13 @@ static void engine_free(tdf_engine *e) {
           e->sky_done[k] = e->spin_done[k] = nullptr;
      }
      if (e->fork_ev) cudaEventDestroy(e->fork_ev);
-     if (e->join_ev) cudaEventDestroy(e->join_ev);
-     e->fork_ev = e->join_ev = nullptr;
-     if (e->lane_own) cudaStreamDestroy(e->lane_own);
-     e->lane_own = nullptr;
+     e->fork_ev = nullptr;
+     for (int l = 0; l < tdf_engine::kMaxLanes; l++) {
+          if (e->join_ev[l]) cudaEventDestroy(e->join_ev[l]);
+          if (e->lane_own[l]) cudaStreamDestroy(e->lane_own[l]);
+          e->join_ev[l] = nullptr;
+          e->lane_own[l] = nullptr;
+     }
      if (e->sky_stream) cudaStreamDestroy(e->sky_stream);
      e->sky_stream = nullptr;
      if (e->own) cudaStreamDestroy(e->own);
@@ -745,7 +777,11 @@ static int run_sky_stage(tdf_engine *e, int npts) {
 // Spindown stage, FFT part, for chunk `ci` of a resolve group whose templates
 // start at dtp: the column pass (demodulation + first FFT pass) and the row
 // pass (second FFT pass + F + candidate bins) for nt templates.
-static cudaStream_t lane_stream(const tdf_engine *e, int l) { return l == 0 ? e->stream : e->lane_own; }
+static cudaStream_t lane_stream(const tdf_engine *e, int l) { return l == 0 ? e->stream : e->lane_own[l]; }
+
+// templates whose F spectra share one trigger-selection launch: whole chunks,
+// at most Gt templates (one chunk when a chunk is larger)
+static int group_templates(const tdf_engine *e) { return std::max(1, e->Gt / e->Tc) * e->Tc; }
 
 template <typename T>
 static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt) {
@@ -757,7 +793,7 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
      const FFTTables<T> &t = *tb;
      const int boff = ci * e->Tc;
      const TmplParam *ctp = dtp + boff;
-     const unsigned G = (unsigned)kGroup * e->Tc;
+     const unsigned G = (unsigned)group_templates(e);
      unsigned *tcnt = Ln.tcnt.as<unsigned>();
      StoreFourstep<T, -1, 2> epi{Ln.Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
      size_t tev = e->timing ? timing_begin(e, st) : (size_t)-1;
@@ -806,7 +842,7 @@ static int run_resolve(tdf_engine *e, int l, const TmplParam *dtp, int ntg) {
      cudaStream_t st = lane_stream(e, l);
      tdf_engine::Lane &Ln = e->ln[l];
      const bool split = std::is_same<T, float>::value;
-     const unsigned G = (unsigned)kGroup * e->Tc;
+     const unsigned G = (unsigned)group_templates(e);
      unsigned *tcnt = Ln.tcnt.as<unsigned>();
      const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
      unsigned long long *cnt = e->counters[e->cur].as<unsigned long long>();
@@ -847,16 +883,16 @@ static int run_resolve(tdf_engine *e, int l, const TmplParam *dtp, int ntg) {
 }
 
 // The spindown stage of nt templates starting at dtp: resolve groups of
-// chunks, group k on lane k % nlanes.  Lane 1 starts after everything queued
-// on the engine stream so far (sky stage, template upload) and the engine
-// stream waits for it at the end, so callers see one ordered stream.
+// chunks, group k on lane k % nlanes.  Lanes 1.. start after everything
+// queued on the engine stream so far (sky stage, template upload) and the
+// engine stream waits for them at the end, so callers see one ordered stream.
 static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
-     const int G = kGroup * e->Tc;
+     const int G = group_templates(e);
      const int ngroups = (nt + G - 1) / G;
      const int lanes = std::min(e->nlanes, ngroups);
      if (lanes > 1) {
           CUCHK(cudaEventRecord(e->fork_ev, e->stream));
-          CUCHK(cudaStreamWaitEvent(e->lane_own, e->fork_ev, 0));
+          for (int l = 1; l < lanes; l++) CUCHK(cudaStreamWaitEvent(e->lane_own[l], e->fork_ev, 0));
      }
      for (int gi = 0; gi < ngroups; gi++) {
           const int g0 = gi * G;
@@ -870,10 +906,67 @@ static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
           if (e->form == TDF_FORM_SPLIT) TRY(run_resolve<float>(e, l, dtp + g0, ntg));
           else TRY(run_resolve<double>(e, l, dtp + g0, ntg));
      }
-     if (lanes > 1) {
-          CUCHK(cudaEventRecord(e->join_ev, e->lane_own));
-          CUCHK(cudaStreamWaitEvent(e->stream, e->join_ev, 0));
+     for (int l = 1; l < lanes; l++) {
+          CUCHK(cudaEventRecord(e->join_ev[l], e->lane_own[l]));
+          CUCHK(cudaStreamWaitEvent(e->stream, e->join_ev[l], 0));
      }
+     return TDF_OK;
+}
+
+// The spindown stage of the current batch (nt templates uploaded to tparam):
+// the first time a configuration is seen its kernels are launched one by one;
+// the second time they are captured (all lanes) into a graph, which later
+// batches with the same configuration replay with one launch.
+static int run_templates_batch(tdf_engine *e, int nt) {
+     const TmplParam *dtp = e->tparam.as<TmplParam>();
+     if (!e->use_graphs || e->timing) return run_templates(e, dtp, nt);
+     const tdf_engine::GraphKey k{e->cur, nt, e->Tc, e->Gt, e->nlanes, e->tparam.p, e->trig[e->cur].p, e->trig_cap};
+     size_t gi = e->graphs.size();
+     for (size_t i = 0; i < e->graphs.size(); i++)
+          if (e->graphs[i].key == k) gi = i;
+     if (gi == e->graphs.size()) {
+          if (e->graphs.size() >= tdf_engine::kMaxGraphs) {
+               size_t old = 0;
+               for (size_t i = 1; i < e->graphs.size(); i++)
+                    if (e->graphs[i].last < e->graphs[old].last) old = i;
+               if (e->graphs[old].exec) cudaGraphExecDestroy(e->graphs[old].exec);
+               e->graphs.erase(e->graphs.begin() + old);
+          }
+          e->graphs.push_back(tdf_engine::GraphEntry());
+          gi = e->graphs.size() - 1;
+          e->graphs[gi].key = k;
+     }
+     tdf_engine::GraphEntry &g = e->graphs[gi];
+     g.last = ++e->graph_tick;
+     if (!g.exec && ++g.seen < 2) return run_templates(e, dtp, nt);
+     if (!g.exec) {
+          if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+               // e.g. the legacy default stream: no capture, plain launches from now on
+               cudaGetLastError();
+               e->use_graphs = false;
+               return run_templates(e, dtp, nt);
+          }
+          const int64_t l0 = e->launches;
+          const int st = run_templates(e, dtp, nt);
+          cudaGraph_t graph = nullptr;
+          const cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+          if (st != TDF_OK || ce != cudaSuccess) {
+               if (graph) cudaGraphDestroy(graph);
+               e->launches = l0;
+               return st != TDF_OK ? st : set_error(TDF_ERR_CUDA, "stream capture: %s", cudaGetErrorString(ce));
+          }
+          const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+          cudaGraphDestroy(graph);
+          if (ie != cudaSuccess) {
+               g.exec = nullptr;
+               e->launches = l0;
+               return set_error(TDF_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ie));
+          }
+          g.launches = e->launches - l0;
+          e->launches = l0;
+     }
+     CUCHK(cudaGraphLaunch(g.exec, e->stream));
+     e->launches += g.launches;
      return TDF_OK;
 }
 
@@ -1000,7 +1093,7 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
                if (e->timing) timing_end(e, sev, KT_SKY, nb, sst);
                CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[slot], 0));
                CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[slot], nt * sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
-               TRY(run_templates(e, e->tparam.as<TmplParam>(), nt));
+               TRY(run_templates_batch(e, nt));
                CUCHK(cudaEventRecord(e->spin_done[slot], e->stream));
                CUCHK(cudaMemcpyAsync(e->h_cnt + 2 * slot, e->counters[slot].p, 2 * sizeof(unsigned long long),
                                      cudaMemcpyDeviceToHost, e->stream));
@@ -1150,7 +1243,11 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      const char *ov = getenv("TDF_SKY_OVERLAP");
      e->overlap = ov && atoi(ov) != 0;   // measured: off is faster when the spindown kernels fill the GPU
      const char *nl = getenv("TDF_LANES");
-     if (nl && atoi(nl) == 1) e->nlanes = 1;
+     if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
+     const char *gr = getenv("TDF_GRAPHS");
+     if (gr && gr[0] == '0') e->use_graphs = false;
+     const char *gt = getenv("TDF_GROUP_TEMPLATES");
+     if (gt && atoi(gt) > 0) e->Gt = atoi(gt);
      autotune_cache_lookup(e);
      e->lines.assign(opts->lines, opts->lines + 2 * (size_t)opts->numlines);
      e->opts.lines = nullptr;
@@ -1158,9 +1255,11 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      int st = TDF_OK;
      cudaError_t ce = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking);
      if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->sky_stream, cudaStreamNonBlocking);
-     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->lane_own, cudaStreamNonBlocking);
      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
-     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join_ev, cudaEventDisableTiming);
+     for (int l = 1; l < e->nlanes && ce == cudaSuccess; l++) {
+          ce = cudaStreamCreateWithFlags(&e->lane_own[l], cudaStreamNonBlocking);
+          if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join_ev[l], cudaEventDisableTiming);
+     }
      for (int k = 0; k < 2 && ce == cudaSuccess; k++) {
           ce = cudaEventCreateWithFlags(&e->sky_done[k], cudaEventDisableTiming);
           if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->spin_done[k], cudaEventDisableTiming);
@@ -1201,7 +1300,8 @@ int tdf_engine_destroy(tdf_engine *e) {
      if (!e) return TDF_OK;
      cudaSetDevice(e->dev);
      if (e->sky_stream) cudaStreamSynchronize(e->sky_stream);
-     if (e->lane_own) cudaStreamSynchronize(e->lane_own);
+     for (cudaStream_t ls : e->lane_own)
+          if (ls) cudaStreamSynchronize(ls);
      if (e->stream) cudaStreamSynchronize(e->stream);
      engine_free(e);
      delete e;
@@ -1380,7 +1480,7 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
                         int32_t *best) {
      if (!e) return set_error(TDF_ERR_INVALID, "null engine");
      CUCHK(cudaSetDevice(e->dev));
-     static const int cands[] = {8, 12, 16, 20, 24, 28, 32, 37, 41, 48};
+     static const int cands[] = {6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 37, 41, 48};
      cudaEvent_t a, b;
      CUCHK(cudaEventCreate(&a));
      CUCHK(cudaEventCreate(&b));
@@ -1395,7 +1495,9 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
           if (c > e->TcMax) continue;
           e->Tc = c;
           float ms = 0.f, m2 = 1e30f;
-          for (int rep = 0; rep < 2 && st == TDF_OK; rep++) {
+          // with graphs: plain launches, capture, replay (a replay is what a search runs)
+          const int reps = e->use_graphs ? 3 : 2;
+          for (int rep = 0; rep < reps && st == TDF_OK; rep++) {
                cudaEventRecord(a, e->stream);
                st = search_core(e, npts, pm, mm, nn, nullptr, pts, tm, false, &ntrig);
                cudaEventRecord(b, e->stream);
@@ -1416,6 +1518,7 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
           return st;
      }
      e->Tc = best_tc;
+     graphs_clear(e);   // the candidates' graphs
      autotune_cache_store(e);
      if (best) *best = best_tc;
      return TDF_OK;

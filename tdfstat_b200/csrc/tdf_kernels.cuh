@@ -439,12 +439,13 @@ struct DemodSplitStaged {
           if (threadIdx.x == 0)
                for (int g = 0; g < stages; g++) issue<L>(g, g, ring, bars, slot_bytes, xbytes, x0, (int)P.slot);
           bool waited = true;
+          int s = 0;            // ring slot of group m
+          unsigned par = 0u;    // phase parity of that slot's barrier
 #pragma unroll
           for (int m = 0; m < 8; m++) {
                float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
                if (m < groups) {
-                    const int s = m % stages;
-                    waited &= mbar_wait(&bars[s], (unsigned)(m / stages) & 1u);
+                    waited &= mbar_wait(&bars[s], par);
                     const unsigned char *sl = ring + (size_t)s * slot_bytes;
                     const float4 *X = reinterpret_cast<const float4 *>(sl);
                     const float *S2 = reinterpret_cast<const float *>(sl + xbytes);
@@ -482,6 +483,10 @@ struct DemodSplitStaged {
                          __syncthreads();
                          if (threadIdx.x == 0)
                               issue<L>(m + stages, s, ring, bars, slot_bytes, xbytes, x0, (int)P.slot);
+                    }
+                    if (++s == stages) {
+                         s = 0;
+                         par ^= 1u;
                     }
                }
                v[0][m] = fa;

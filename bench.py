@@ -231,7 +231,11 @@ def run_tdf(args, rank, world, local_rank):
         # chunk size by the engine's autotuner on a 16-point sample (untimed)
         tuned = eng.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
         # warm-up (kernels are compiled ahead of time for sm_100a)
+        # warm-up steps are the timed step exactly (the flush included: its
+        # first launch loads torch's fill kernel)
         for _ in range(args.warmup):
+            with torch.cuda.stream(stream):
+                flush.zero_()
             eng.search_device(pm, mm, nn)
         torch.cuda.synchronize()
         # ---- value: device-resident inputs, K steps

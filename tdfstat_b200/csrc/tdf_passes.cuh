@@ -21,10 +21,16 @@ constexpr size_t pass_smem_bytes() {
      return sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
 }
 
-// resident CTAs per SM the FP32 passes are compiled for (register cap)
+// resident CTAs per SM the FP32 passes are compiled for (register cap):
+// column passes, and row passes (which hold no demodulation operands and fit
+// 64 registers at L <= 256 without spilling)
 template <typename T, int L>
 constexpr int pass_min_blocks() {
      return sizeof(T) == 4 ? (L <= 256 ? 3 : (L == 512 ? 2 : 1)) : 1;
+}
+template <typename T, int L>
+constexpr int row_min_blocks() {
+     return sizeof(T) == 4 ? (L <= 256 ? 4 : (L == 512 ? 2 : 1)) : 1;
 }
 
 // A prologue with `static constexpr bool kStaged = true` stages its operands
@@ -62,7 +68,7 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
 }
 
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
-__global__ void __launch_bounds__(L, (pass_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
+__global__ void __launch_bounds__(L, (row_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
      extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);

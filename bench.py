@@ -21,8 +21,10 @@ A step is one pass of the hot path over the whole patch.  Inputs are synthetic
   --impl reference: the reference's own C search (its unmodified sources,
           PREC=FLOAT, built by oracle/Makefile) on the host cores, each step
           a bounded sample (2 sky points x 401 spindowns) of the workload.
-Under torchrun (N > 1) the sky points are split into contiguous shards, one
-per rank (no collective on the data path); rank 0 prints the JSON line.
+Under torchrun (N > 1) every rank searches its own 32 x 32 patch (the same
+region, shifted by a fraction of a grid step per rank) as a contiguous shard
+of one point list: weak scaling, no collective on the data path; the
+whole-job value counts all ranks' templates; rank 0 prints the JSON line.
 """
 from __future__ import annotations
 
@@ -54,17 +56,26 @@ def workload_case(name: str):
     if name == "cfg1":
         return synth.Case(dt=2.0, nod=2, band=2880, dets=("H1",), read_o3=True, seed=101, thr=14.5,
                           fdot_step=1e-10, sky_cells=16.0), (1, 1), 64, 0.25
+    # the injections (and the patches centred on them) lie well inside the
+    # sky grid's ellipse: every patch point is searched (job_core skips
+    # points outside it, jobcore.c:248)
     if name == "cfg3":
-        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=1.9, dec=0.2, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
         return synth.Case(dt=2.0, nod=6, band=2880, dets=("H1", "L1"), seed=303, thr=14.5, fdot_step=1e-10,
-                          sky_cells=16.0, injections=(inj,)), (128, 64), 401, 0.25
-    inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=1.9, dec=0.2, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+                          sky_cells=16.0, injections=(inj,)), (128, 64), 401, 0.1
+    inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
     return synth.Case(dt=2.0, nod=2, band=2880, dets=("H1", "L1"), seed=202, thr=14.5, fdot_step=1e-10,
                       sky_cells=16.0, injections=(inj,)), (32, 32), 401, 0.25
 
 
 class Workload:
-    def __init__(self, name: str, root: str):
+    """The benchmark search: one sky patch x nspd spindowns per rank.  With
+    `world` ranks the point list holds world patches of the same region,
+    patch r shifted by r/world of a grid step in mm (distinct sky points,
+    all inside the grid), so that each rank's contiguous shard is one full
+    patch: the work per GPU is fixed as the GPU count grows."""
+
+    def __init__(self, name: str, root: str, world: int = 1):
         from tdfstat_b200 import host, synth
         case, (nm, nn_), nspd, step = workload_case(name)
         self.name, self.case = name, case
@@ -88,10 +99,14 @@ class Workload:
         job.sett.bufsize = job.sett.nfftf
         pm0, mm0, nn0 = job.sky_points()
         m0, n0 = mm0[0], nn0[0]
-        self.pm = np.full(nm * nn_, pm0[0], dtype=np.int32)
-        mg, ng = np.meshgrid((np.arange(nm) - nm // 2) * step, (np.arange(nn_) - nn_ // 2) * step, indexing="ij")
-        self.mm = (m0 + mg.ravel()).astype(np.float32)
-        self.nn = (n0 + ng.ravel()).astype(np.float32)
+        pms, mms, nns = [], [], []
+        for r in range(world):
+            mg, ng = np.meshgrid((np.arange(nm) - nm // 2 + r / world) * step, (np.arange(nn_) - nn_ // 2) * step,
+                                 indexing="ij")
+            pms.append(np.full(nm * nn_, pm0[0], dtype=np.int32))
+            mms.append((m0 + mg.ravel()).astype(np.float32))
+            nns.append((n0 + ng.ravel()).astype(np.float32))
+        self.pm, self.mm, self.nn = np.concatenate(pms), np.concatenate(mms), np.concatenate(nns)
         self.nspd = nspd
         self.templates = nm * nn_ * nspd
         self.config = {"workload": name, "detectors": "".join(c.dets), "N": job.sett.N, "nfft": job.sett.nfft,
@@ -210,18 +225,17 @@ def run_tdf(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     root = tempfile.mkdtemp(prefix="tdfbench_")
     try:
-        wl = Workload(args.workload, root)
-        if args.sky_points:
-            wl.pm, wl.mm, wl.nn = wl.pm[:args.sky_points], wl.mm[:args.sky_points], wl.nn[:args.sky_points]
-            wl.config["sky_points"] = len(wl.pm)
-            wl.config["templates_per_step"] = len(wl.pm) * wl.nspd
+        wl = Workload(args.workload, root, world)
         job = wl.job
         pm, mm, nn = wl.shard(rank, world)
+        if args.sky_points:
+            pm, mm, nn = pm[:args.sky_points], mm[:args.sky_points], nn[:args.sky_points]
+            wl.config["sky_points"] = len(pm)
+            wl.config["templates_per_step"] = len(pm) * wl.nspd
         seg, opts = job.segment(), job.search_opts()
         eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
         lib = load_library()
         stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
-        ntmpl = len(pm) * wl.nspd
         flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
         def barrier():
@@ -230,7 +244,6 @@ def run_tdf(args, rank, world, local_rank):
 
         # chunk size by the engine's autotuner on a 16-point sample (untimed)
         tuned = eng.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
-        # warm-up (kernels are compiled ahead of time for sm_100a)
         # warm-up steps are the timed step exactly (the flush included: its
         # first launch loads torch's fill kernel)
         for _ in range(args.warmup):
@@ -238,6 +251,12 @@ def run_tdf(args, rank, world, local_rank):
                 flush.zero_()
             eng.search_device(pm, mm, nn)
         torch.cuda.synchronize()
+        # templates a step searches = records it writes (one per spindown of
+        # every point inside the grid ellipse)
+        ntmpl, _ = eng.search_device(pm, mm, nn)
+        if ntmpl != len(pm) * wl.nspd:
+            print("bench: %d of %d patch templates lie inside the sky grid" % (ntmpl, len(pm) * wl.nspd),
+                  file=sys.stderr)
         # ---- value: device-resident inputs, K steps
         launches0 = eng.launch_count()
         clocks = ClockSampler(local_rank)
@@ -246,12 +265,14 @@ def run_tdf(args, rank, world, local_rank):
         torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ntrig = 0
+        nsearched = 0
         ev0.record(stream)
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()   # 256 MiB (> L2) written between steps, on the engine's stream
             nrec, nt = eng.search_device(pm, mm, nn)
             ntrig += nt
+            nsearched += nrec
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -276,9 +297,11 @@ def run_tdf(args, rank, world, local_rank):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        nsearched_e2e = 0
         for _ in range(args.steps):
             eng.upload(seg)
             res = eng.search(pm, mm, nn)
+            nsearched_e2e += len(res)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -286,14 +309,15 @@ def run_tdf(args, rank, world, local_rank):
         h2d = sum(d.xdat.nbytes + d.detssb.nbytes for d in job.dets) + job.cosmodf.nbytes + job.sinmodf.nbytes \
             + pm.nbytes + mm.nbytes + nn.nbytes
         d2h = len(res) * 40 + res.pairs_flat.nbytes
-        # max over ranks
+        # times: max over ranks; templates searched: sum over ranks
         t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+        n = torch.tensor([nsearched, nsearched_e2e], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dist.all_reduce(n, op=dist.ReduceOp.SUM)
         ms, ms_e2e = float(t[0]), float(t[1])
-        total_tmpl = len(wl.pm) * wl.nspd
-        value = total_tmpl * args.steps / (ms / 1e3)
-        e2e = total_tmpl * args.steps / (ms_e2e / 1e3)
+        value = float(n[0]) / (ms / 1e3)
+        e2e = float(n[1]) / (ms_e2e / 1e3)
         out = None
         if rank == 0:
             peak, peak_kind = measured_peaks()
@@ -328,10 +352,12 @@ def run_tdf(args, rank, world, local_rank):
             out = {
                 "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-                "scaling": "weak" if world > 1 else "weak", "vs_baseline": None,
+                "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
                 "data": "synthetic (seeded Gaussian noise + injected CW signal, synthetic ephemeris)",
                 "config": dict(wl.config, form=args.form, templates_per_chunk=tuned,
+                               templates_searched_per_step_per_gpu=int(ntmpl),
+                               templates_searched_per_step=int(round(float(n[0]) / args.steps)),
                                l2="flush: 256 MiB write between timed steps; per-step working set > L2"),
                 "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},

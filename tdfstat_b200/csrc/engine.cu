@@ -889,7 +889,8 @@ static int run_resolve(tdf_engine *e, int l, const TmplParam *dtp, int ntg) {
 static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
      const int G = group_templates(e);
      const int ngroups = (nt + G - 1) / G;
-     const int lanes = std::min(e->nlanes, ngroups);
+     // per-kernel event timing measures kernels one after another: one lane
+     const int lanes = e->timing ? 1 : std::min(e->nlanes, ngroups);
      if (lanes > 1) {
           CUCHK(cudaEventRecord(e->fork_ev, e->stream));
           for (int l = 1; l < lanes; l++) CUCHK(cudaStreamWaitEvent(e->lane_own[l], e->fork_ev, 0));

@@ -91,9 +91,16 @@ static int set_smem(K kern, size_t smem) {
 }
 
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
-static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
+static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T> *tw, cudaStream_t st) {
      size_t smem = pass_smem_bytes<T, L, NA>();
      if constexpr (is_staged<Pro>::value) smem = pro.smem;
+     Epi epi = epi_in;
+     if constexpr (has_tables<Epi>::value) {
+          // the epilogue's tables go after everything else
+          smem = (smem + 15) / 16 * 16;
+          epi.tab_off = (unsigned)smem;
+          smem += Epi::template table_bytes<L>(epi.N2);
+     }
      auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi>;
      TRY(set_smem(kern, smem));
      kern<<<grid, L, smem, st>>>(pro, epi, tw);
@@ -472,7 +479,9 @@ static int staged_setup(tdf_engine *e) {
      const size_t bars = 8 * sizeof(uint64_t);
      const int rows = (e->N + N2 - 1) / N2;
      const int groups = std::min(8, (rows + R - 1) / R);
-     const size_t budget = std::min<size_t>(227 * 1024, 233472 / blocks - 1024);
+     // less the epilogue's twiddle tables (StoreFourstep), which follow the ring
+     const size_t tables = sizeof(float2) * ((size_t)L * N2 / 1024 + 1024) + 16;
+     const size_t budget = std::min<size_t>(227 * 1024, 233472 / blocks - 1024) - tables;
      if (budget < tw + bars + slot) return TDF_OK;
      const int stages = (int)std::min<size_t>((size_t)groups, (budget - tw - bars) / slot);
      const size_t area = std::max(lines, (size_t)stages * slot);

@@ -237,4 +237,10 @@ __device__ __forceinline__ cx<T> fourstep_twiddle(const cx<T> *__restrict__ hi, 
      return cmul(a, b);
 }
 
+// the same from copies of the tables in shared memory
+template <typename T>
+__device__ __forceinline__ cx<T> fourstep_twiddle_smem(const cx<T> *hi, const cx<T> *lo, int m) {
+     return cmul(hi[m >> 10], lo[m & 1023]);
+}
+
 }  // namespace tdf

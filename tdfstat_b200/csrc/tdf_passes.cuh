@@ -41,6 +41,14 @@ struct is_staged : std::false_type {};
 template <class P>
 struct is_staged<P, std::void_t<decltype(P::kStaged)>> : std::integral_constant<bool, P::kStaged> {};
 
+// An epilogue with `static constexpr bool kTables = true` keeps tables in
+// dynamic shared memory at byte offset tab_off: load_tables<L>() fills them
+// before the first barrier and store() gets the shared memory base.
+template <class P, class = void>
+struct has_tables : std::false_type {};
+template <class P>
+struct has_tables<P, std::void_t<decltype(P::kTables)>> : std::integral_constant<bool, P::kTables> {};
+
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
 __global__ void __launch_bounds__(L, (pass_min_blocks<T, L>()))
 k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
@@ -49,6 +57,7 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
      load_table<T>(tw, twline, L);
+     if constexpr (has_tables<Epi>::value) epi.template load_tables<L>(smem_raw);
      const int tid = threadIdx.x;
      const int c = tid % LINES, t = tid / LINES;
      const int n2 = blockIdx.x * LINES + c;
@@ -64,7 +73,10 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
      for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
      __syncthreads();
      line_fft<T, L, SIGN, NA>(v, s, tw, t);
-     epi.template store<L>(v, b, n2, t);
+     if constexpr (has_tables<Epi>::value)
+          epi.template store<L>(v, b, n2, t, smem_raw);
+     else
+          epi.template store<L>(v, b, n2, t);
 }
 
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
@@ -96,18 +108,48 @@ __global__ void __launch_bounds__(L, (row_min_blocks<T, L>())) k_rowpass(Src src
 // Batch b's arrays are interleaved element by element: array a of element e
 // lives at y[((size_t)b*N + e)*NA + a], so both arrays of a sample move in one
 // access (16 bytes for two float2).
+// The twiddle tables hi[L*N2/1024] = W^(1024 i), lo[1024] = W^j are copied
+// into dynamic shared memory at byte offset tab_off (set by the launcher) when
+// the kernel starts, in the same batch of loads as the line table.  FP32
+// passes form a thread's eight twiddles W^(n2 (t + m L/8)) by recurrence from
+// W^(n2 t) and W^(n2 L/8) (relative error below 1e-6); FP64 passes look each
+// one up.
 template <typename T, int SIGN, int NA>
 struct StoreFourstep {
      cx<T> *y;
      const cx<T> *hi, *lo;
      int N2;
-     int N;
+     int N;                 // array stride
+     unsigned tab_off = 0;  // byte offset of the shared copies of hi, lo
+     static constexpr bool kTables = true;
+
      template <int L>
-     __device__ __forceinline__ void store(const cx<T> (&v)[NA][8], int b, int n2, int t) const {
+     __host__ __device__ static constexpr int nhi(int N2) { return L * N2 / 1024; }
+     template <int L>
+     __host__ __device__ static size_t table_bytes(int N2) { return sizeof(cx<T>) * (size_t)(nhi<L>(N2) + 1024); }
+
+     template <int L>
+     __device__ __forceinline__ void load_tables(unsigned char *smem) const {
+          cx<T> *s = reinterpret_cast<cx<T> *>(smem + tab_off);
+          const int nh = nhi<L>(N2);
+          for (int i = threadIdx.x; i < nh + 1024; i += blockDim.x) s[i] = i < nh ? __ldg(&hi[i]) : __ldg(&lo[i - nh]);
+     }
+
+     template <int L>
+     __device__ __forceinline__ void store(const cx<T> (&v)[NA][8], int b, int n2, int t, unsigned char *smem) const {
+          const cx<T> *hs = reinterpret_cast<const cx<T> *>(smem + tab_off);
+          const cx<T> *ls = hs + nhi<L>(N2);
+          cx<T> w = twsign<SIGN>(fourstep_twiddle_smem<T>(hs, ls, n2 * t));
+          cx<T> st = w;
+          if constexpr (sizeof(T) == 4) st = twsign<SIGN>(fourstep_twiddle_smem<T>(hs, ls, n2 * (L / 8)));
 #pragma unroll
           for (int m = 0; m < 8; m++) {
                const int k1 = t + m * (L / 8);
-               const cx<T> w = twsign<SIGN>(fourstep_twiddle<T>(hi, lo, n2 * k1));   // shared by the arrays
+               if constexpr (sizeof(T) == 4) {
+                    if (m > 0) w = cmul(w, st);
+               } else {
+                    w = twsign<SIGN>(fourstep_twiddle_smem<T>(hs, ls, n2 * k1));
+               }
                cx<T> *dst = y + ((size_t)b * N + n2 + (size_t)k1 * N2) * NA;
                if constexpr (NA == 2 && sizeof(T) == 4) {
                     const cx<T> p = cmul(v[0][m], w), q = cmul(v[1][m], w);

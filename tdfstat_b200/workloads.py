@@ -1,0 +1,85 @@
+"""The synthetic workloads of the benchmark and of the full-size GPU tests.
+
+  cfg1  H1, N = 86164 (2 sidereal days at dt = 2 s), float64 input
+        (mods=read_O3), one sky point x 64 spindowns
+  cfg2  H1+L1, N = 86164, nfft = nfftf = 2^17, Ninterp = 2^18, Gaussian noise
+        (sigma 1, 5% gaps) + a CW injection (network SNR 12, 100.1234 Hz,
+        -3e-10 Hz/s), a 32 x 32 sky patch around the injection (step 0.25
+        grid cells) x 401 spindowns = 410,624 templates
+  cfg3  as cfg2 with N = 258492 (6 days), nfft = 2^18, Ninterp = 2^19,
+        a 128 x 64 patch (step 0.1 cells) x 401 spindowns = 3,284,992 templates
+All are seeded; the F range is the all-sky one, [nmin, nmax] (settings.c:83-84).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import host, synth
+from .shard import shard_points
+
+
+def workload_case(name: str):
+    if name == "cfg1":
+        return synth.Case(dt=2.0, nod=2, band=360, dets=("H1",), read_o3=True, seed=101, thr=14.5,
+                          fdot_step=1e-10, sky_cells=16.0), (1, 1), 64, 0.25
+    # the injections (and the patches centred on them) lie well inside the
+    # sky grid's ellipse: every patch point is searched (job_core skips
+    # points outside it, jobcore.c:248)
+    if name == "cfg3":
+        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+        return synth.Case(dt=2.0, nod=6, band=360, dets=("H1", "L1"), seed=303, thr=14.5, fdot_step=1e-10,
+                          sky_cells=16.0, injections=(inj,)), (128, 64), 401, 0.1
+    inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+    return synth.Case(dt=2.0, nod=2, band=360, dets=("H1", "L1"), seed=202, thr=14.5, fdot_step=1e-10,
+                      sky_cells=16.0, injections=(inj,)), (32, 32), 401, 0.25
+
+
+class Workload:
+    """The benchmark search: one sky patch x nspd spindowns per rank.  With
+    `world` ranks the point list holds world patches of the same region,
+    patch r shifted by r/world of a grid step in mm (distinct sky points,
+    all inside the grid), so that each rank's contiguous shard is one full
+    patch: the work per GPU is fixed as the GPU count grows."""
+
+    def __init__(self, name: str, root: str, world: int = 1):
+        case, (nm, nn_), nspd, step = workload_case(name)
+        self.name, self.case = name, case
+        inj = case.injections[0] if case.injections else None
+        c = case
+        # a directed_range INI centred on the injection (or a fixed point)
+        ra, dec = (inj.ra, inj.dec) if inj else (1.2, 0.3)
+        fdot = inj.fdot if inj else 0.0
+        st = c.settings()
+        c.gtype = "directed_range"
+        c.gcenter = (st.fpo + st.B / 2, fdot, ra, dec)
+        half = (nspd - 1) // 2
+        c.gsizes = (st.nfft // 4 - 1024, float(half), 0.0, 0.0)
+        c.gsteps = (1, 1.0, 1.0, 1.0)
+        ini = synth.write_case(root, c)
+        self.ini = ini
+        job = host.Job(ini, float_build=True)
+        self.job = job
+        # the F range of an all-sky run: [nmin, nmax]
+        job.range.fr = [job.sett.nmin, job.sett.nmax]
+        job.sett.bufsize = job.sett.nfftf
+        pm0, mm0, nn0 = job.sky_points()
+        m0, n0 = mm0[0], nn0[0]
+        pms, mms, nns = [], [], []
+        for r in range(world):
+            mg, ng = np.meshgrid((np.arange(nm) - nm // 2 + r / world) * step, (np.arange(nn_) - nn_ // 2) * step,
+                                 indexing="ij")
+            pms.append(np.full(nm * nn_, pm0[0], dtype=np.int32))
+            mms.append((m0 + mg.ravel()).astype(np.float32))
+            nns.append((n0 + ng.ravel()).astype(np.float32))
+        self.pm, self.mm, self.nn = np.concatenate(pms), np.concatenate(mms), np.concatenate(nns)
+        self.nspd = nspd
+        self.shape = (nm, nn_)
+        self.centre = (nm // 2) * nn_ + nn_ // 2   # index of the patch centre (the injection's grid point)
+        self.templates = nm * nn_ * nspd
+        self.config = {"workload": name, "detectors": "".join(c.dets), "N": job.sett.N, "nfft": job.sett.nfft,
+                       "nfftf": job.sett.nfftf, "Ninterp": job.sett.Ninterp, "sky_points": nm * nn_,
+                       "spindowns": nspd, "templates_per_step": self.templates,
+                       "fr": list(job.range.fr), "thr": c.thr}
+
+    def shard(self, rank: int, world: int):
+        return shard_points(self.pm, self.mm, self.nn, rank, world)

@@ -214,7 +214,13 @@ def run_tdf(args, rank, world, local_rank):
         ms = ev0.elapsed_time(ev1)
         launches = eng.launch_count() - launches0
         # ---- per-kernel durations: the same K steps again with CUDA events
-        # recorded on the engine's stream around every launch
+        # recorded on the engine's stream around every launch.  Timing runs
+        # the kernels one after another (one lane); each launch gets at
+        # least 32 templates (1024 column-pass CTAs, 3.5 waves at 2 per SM)
+        # so that a launch has the GPU to itself rather than under-filling it
+        tc_run = eng.templates_per_chunk
+        tc_timed = max(tc_run, 32)
+        eng.templates_per_chunk = tc_timed
         eng.enable_kernel_timing(True)
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
@@ -223,6 +229,7 @@ def run_tdf(args, rank, world, local_rank):
         torch.cuda.synchronize()
         ktimes = eng.kernel_times()
         eng.enable_kernel_timing(False)
+        eng.templates_per_chunk = tc_run
         # ---- e2e: host buffers through the C ABI
         for _ in range(1):
             eng.upload(seg)
@@ -272,7 +279,9 @@ def run_tdf(args, rank, world, local_rank):
                         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                         "algorithmic_bytes_per_template": bt,
                         "kernel_ms_share": {k: round(v, 3) for k, v in ktimes.items() if k.endswith("_ms")},
-                        "avg_launch_ms": round(col_ms / col_n, 4), "templates_per_launch": col_t / col_n}
+                        "avg_launch_ms": round(col_ms / col_n, 4), "templates_per_launch": col_t / col_n,
+                        "timed": "CUDA events on the engine stream around each launch, one lane, %d templates "
+                                 "per launch (the run itself: %d per chunk over concurrent lanes)" % (tc_timed, tc_run)}
             cpu = None
             if not args.no_cpu_baseline:
                 r = cpu_reference_sample(wl, tempfile.mkdtemp(prefix="tdfcpu_"), 3, os.cpu_count() or 1)

@@ -198,12 +198,19 @@ int tdf_engine_get_stream(tdf_engine *e, void **stream);
 int tdf_engine_set_stream(tdf_engine *e, void *stream);
 
 /* Chooses the templates per chunk of the spindown stage by timing a few
-   sizes (8..32) on these points (device-only passes) and keeps the fastest
+   sizes (6..48) on these points (device-only passes) and keeps the fastest
    in the engine; *best (may be NULL) receives it.  With the environment
    variable TDF_AUTOTUNE_CACHE=<file> the choice is appended to that file and
    picked up by engines created later for the same form, sizes and GPU. */
 int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
                         int32_t *best);
+
+/* Templates per chunk of the spindown stage (one column-pass and one
+   row-pass launch each): get, and set to 1..48 (TDF_ERR_INVALID otherwise).
+   tdf_engine_autotune() chooses it; a set value holds until the next
+   autotune.  Extension of this library: job_core() has no chunking. */
+int tdf_engine_get_templates_per_chunk(tdf_engine *e, int32_t *tc);
+int tdf_engine_set_templates_per_chunk(tdf_engine *e, int32_t tc);
 
 /* Kernel launches issued by the engine since creation (for accounting). */
 int tdf_engine_launch_count(tdf_engine *e, int64_t *count);

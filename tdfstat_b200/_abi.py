@@ -130,6 +130,8 @@ ABI_FUNCTIONS = [
     ("tdf_engine_get_stream", C.c_int, [P, C.POINTER(P)]),
     ("tdf_engine_set_stream", C.c_int, [P, P]),
     ("tdf_engine_autotune", C.c_int, [P, C.c_int, I32P, F32P, F32P, I32P]),
+    ("tdf_engine_get_templates_per_chunk", C.c_int, [P, I32P]),
+    ("tdf_engine_set_templates_per_chunk", C.c_int, [P, C.c_int32]),
     ("tdf_engine_launch_count", C.c_int, [P, I64P]),
     ("tdf_engine_set_kernel_timing", C.c_int, [P, C.c_int]),
     ("tdf_engine_get_kernel_times", C.c_int, [P, C.POINTER(TdfKernelTimes)]),

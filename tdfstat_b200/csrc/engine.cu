@@ -1534,6 +1534,21 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
      return TDF_OK;
 }
 
+int tdf_engine_get_templates_per_chunk(tdf_engine *e, int32_t *tc) {
+     if (!e || !tc) return set_error(TDF_ERR_INVALID, "null argument");
+     *tc = e->Tc;
+     return TDF_OK;
+}
+
+int tdf_engine_set_templates_per_chunk(tdf_engine *e, int32_t tc) {
+     if (!e) return set_error(TDF_ERR_INVALID, "null engine");
+     if (tc < 1 || tc > e->TcMax) return set_error(TDF_ERR_INVALID, "templates per chunk %d outside 1..%d", tc, e->TcMax);
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     e->Tc = tc;
+     return TDF_OK;
+}
+
 int tdf_engine_launch_count(tdf_engine *e, int64_t *count) {
      if (!e || !count) return set_error(TDF_ERR_INVALID, "null argument");
      *count = e->launches;

@@ -182,6 +182,16 @@ class Engine:
                                                       _p(nn, C.c_float), C.byref(best)))
         return best.value
 
+    @property
+    def templates_per_chunk(self) -> int:
+        tc = C.c_int32(0)
+        _check(self.lib, self.lib.tdf_engine_get_templates_per_chunk(self.h, C.byref(tc)))
+        return tc.value
+
+    @templates_per_chunk.setter
+    def templates_per_chunk(self, tc: int):
+        _check(self.lib, self.lib.tdf_engine_set_templates_per_chunk(self.h, int(tc)))
+
     def enable_kernel_timing(self, on: bool = True):
         _check(self.lib, self.lib.tdf_engine_set_kernel_timing(self.h, 1 if on else 0))
 

@@ -3,7 +3,7 @@ one on a single stream (TDF_GRAPHS=0, TDF_LANES=1) against the default
 engine, which spreads resolve groups over several lanes and, from the second
 time a batch configuration is seen, replays it as a captured CUDA graph.
 Repeated calls on one engine go through the first-sighting, capture and
-replay paths in turn."""
+replay paths in turn.  Records are also the same for every chunk size."""
 import numpy as np
 import pytest
 
@@ -42,4 +42,20 @@ def test_graph_replay_matches_plain_launches(golden, monkeypatch, name):
         launches.append(eng.launch_count() - n0)
     # a replayed graph counts the kernels it holds
     assert launches[0] == launches[1] == launches[2] > 0
+    eng.close()
+
+
+def test_records_do_not_depend_on_chunk_size(golden):
+    from tdfstat_b200.engine import Engine, TdfError
+    g = golden("g2_h1l1_inj")
+    pm, mm, nn = g.job32.sky_points()
+    eng = Engine.from_job(g.job32, form="split")
+    ref = _records(eng.search(pm, mm, nn))
+    for tc in (1, 3, 17, 48):
+        eng.templates_per_chunk = tc
+        assert eng.templates_per_chunk == tc
+        _same(_records(eng.search(pm, mm, nn)), ref)
+    for bad in (0, 49):
+        with pytest.raises(TdfError):
+            eng.templates_per_chunk = bad
     eng.close()

@@ -109,8 +109,15 @@ static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T
 }
 
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
-static int launch_row_L(dim3 grid, const Src &src, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
-     constexpr size_t smem = pass_smem_bytes<T, L, NA>();
+static int launch_row_L(dim3 grid, const Src &src_in, const Epi &epi, const cx<T> *tw, cudaStream_t st) {
+     size_t smem = pass_smem_bytes<T, L, NA>();
+     Src src = src_in;
+     if constexpr (is_bulk<Src>::value) {
+          // the copies' barrier after the line buffers
+          smem = (smem + 15) / 16 * 16;
+          src.bar_off = (unsigned)smem;
+          smem += 16;
+     }
      auto kern = k_rowpass<T, L, SIGN, NA, Src, Epi>;
      TRY(set_smem(kern, smem));
      kern<<<grid, L, smem, st>>>(src, epi, tw);
@@ -322,6 +329,7 @@ struct tdf_engine {
      std::vector<GraphEntry> graphs;
      uint64_t graph_tick = 0;
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
+     bool row_bulk = true;     // split-form row pass fetches its rows by bulk copies (TDF_ROW_BULK=0: per thread)
      // optional per-kernel event timing
      bool timing = false;
      tdf_kernel_times kt{};
@@ -832,12 +840,23 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
      }
      if (e->timing) timing_end(e, tev, KT_COL, nt, st);
      const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
-     RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
      StoreFstat<T> epi2{Ln.Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF, e->opts.fr[0],
                         e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G,
                         e->cand_cap, boff};
      tev = e->timing ? timing_begin(e, st) : (size_t)-1;
-     TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+     if constexpr (std::is_same<T, float>::value) {
+          if (e->row_bulk) {
+               RowsYBulk src{Ln.Ybuf.as<float2>(), e->nfftf, t.N2,
+                             reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1)};
+               TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+          } else {
+               RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
+               TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+          }
+     } else {
+          RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
+          TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+     }
      if (e->timing) timing_end(e, tev, KT_ROW, nt, st);
      e->launches += 2;
      return TDF_OK;
@@ -1005,7 +1024,7 @@ static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_tot
      if (errf & ERR_OVERFLOW)
           return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
      if (errf & ERR_STAGE_TIMEOUT)
-          return set_error(TDF_ERR_CUDA, "column pass: an operand copy did not complete within the wait limit");
+          return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
      if (nfound > e->trig_cap) {
           *over = true;
           e->h_cnt[2 * slot] = nfound;   // keep the needed size visible
@@ -1256,6 +1275,8 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
      const char *gr = getenv("TDF_GRAPHS");
      if (gr && gr[0] == '0') e->use_graphs = false;
+     const char *rb = getenv("TDF_ROW_BULK");
+     if (rb && rb[0] == '0') e->row_bulk = false;
      const char *gt = getenv("TDF_GROUP_TEMPLATES");
      if (gt && atoi(gt) > 0) e->Gt = atoi(gt);
      autotune_cache_lookup(e);
@@ -1452,7 +1473,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      CUCHK(cudaMemcpyAsync(e->h_cnt, e->counters[0].p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
      CUCHK(cudaStreamSynchronize(e->stream));
      if (e->h_cnt[1] & ERR_STAGE_TIMEOUT)
-          return set_error(TDF_ERR_CUDA, "column pass: an operand copy did not complete within the wait limit");
+          return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
      const int n = e->nF;
      if (e->form == TDF_FORM_SPLIT) {
           std::vector<float> f(n), mu(std::max(1, e->nblk_mu));

@@ -8,6 +8,9 @@
 
 namespace tdf {
 
+// or-ed into a kernel's error word when a bounded wait on a copy gave up
+constexpr unsigned ERR_STAGE_TIMEOUT = 2u;
+
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
      return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -44,6 +47,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int li
           if (done) return true;
      }
      return false;
+}
+
+// 1-D bulk copy of `bytes` (a multiple of 16; both addresses 16-byte
+// aligned) from global to shared memory, completing on `bar` (no multicast).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+     asm volatile(
+         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+             smem_addr(dst)),
+         "l"((uint64_t)src), "r"(bytes), "r"(smem_addr(bar))
+         : "memory");
 }
 
 // Tiled 4-D TMA load of one box into shared memory (no multicast).  The

@@ -59,7 +59,6 @@ struct Trig {
 };
 
 constexpr unsigned ERR_OVERFLOW = 1u;
-constexpr unsigned ERR_STAGE_TIMEOUT = 2u;   // an operand copy did not complete within the wait limit
 constexpr double TWO_PI = 6.283185307179586476925286766559;
 constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
 constexpr double M_PI_D = 3.14159265358979323846;

@@ -12,6 +12,7 @@
 
 #include <type_traits>
 
+#include "tdf_bulk.cuh"
 #include "tdf_fft.cuh"
 
 namespace tdf {
@@ -44,6 +45,15 @@ struct is_staged<P, std::void_t<decltype(P::kStaged)>> : std::integral_constant<
 // An epilogue with `static constexpr bool kTables = true` keeps tables in
 // dynamic shared memory at byte offset tab_off: load_tables<L>() fills them
 // before the first barrier and store() gets the shared memory base.
+// A row-pass source with `static constexpr bool kBulk = true` brings the
+// CTA's rows into shared memory itself: load_bulk() gets the line-buffer
+// area (free until the first pass stores) and its barrier at pro.bar_off,
+// and loads the line twiddle table on the way.
+template <class P, class = void>
+struct is_bulk : std::false_type {};
+template <class P>
+struct is_bulk<P, std::void_t<decltype(P::kBulk)>> : std::integral_constant<bool, P::kBulk> {};
+
 template <class P, class = void>
 struct has_tables : std::false_type {};
 template <class P>
@@ -89,14 +99,19 @@ __global__ void __launch_bounds__(L, (row_min_blocks<T, L>())) k_rowpass(Src src
      const int b = blockIdx.y;
      const int k1b = blockIdx.x * LINES;
      const int c = tid % LINES, t = tid / LINES;
-     // first-pass inputs straight from the rows into registers: per load
-     // instruction a warp reads 4 consecutive elements of each of 8 rows
      cx<T> v[NA][8];
      cx<T> *s[NA];
-     src.template load<L>(v, b, k1b + c, t);
+     if constexpr (is_bulk<Src>::value) {
+          src.template load_bulk<L>(v, b, k1b, c, t, reinterpret_cast<unsigned char *>(lines),
+                                    reinterpret_cast<uint64_t *>(smem_raw + src.bar_off), tw, twline);
+     } else {
+          // first-pass inputs straight from the rows into registers: per load
+          // instruction a warp reads 4 consecutive elements of each of 8 rows
+          src.template load<L>(v, b, k1b + c, t);
+          load_table<T>(tw, twline, L);
+     }
 #pragma unroll
      for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
-     load_table<T>(tw, twline, L);
      __syncthreads();
      line_fft<T, L, SIGN, NA>(v, s, tw, t);
      epi.template store<L>(v, b, k1b + c, t);
@@ -184,6 +199,58 @@ struct RowsY {
                     for (int a = 0; a < NA; a++) v[a][m] = e[a];
                }
           }
+     }
+};
+
+// RowsY for the split form with the CTA's LINES rows brought in by bulk
+// copies: row r (N2 elements of 16 bytes, both arrays) goes to shared offset
+// r * (16*N2 + 64), so that the 8 rows a warp reads from at once fall on
+// alternate halves of the banks; the slots alias the line buffers, which the
+// first pass only writes after the barrier that follows the reads.  Thread
+// 0 issues the copies; everyone waits on one mbarrier (bounded: on time-out
+// ERR_STAGE_TIMEOUT is or-ed into *err).
+struct RowsYBulk {
+     const float2 *y;
+     int N;            // N1*N2
+     int rowstride;    // N2
+     unsigned *err;
+     unsigned bar_off = 0;   // byte offset of the barrier in dynamic shared memory (set by the launcher)
+     static constexpr bool kBulk = true;
+     static constexpr unsigned kPad = 64;
+
+     template <int L>
+     __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)LINES * (16 * L + kPad); }
+
+     template <int L>
+     __device__ __forceinline__ void load_bulk(float2 (&v)[2][8], int b, int k1b, int c, int t, unsigned char *stage,
+                                               uint64_t *bar, float2 *tw, const float2 *twline) const {
+          constexpr unsigned RB = 16 * L;   // bytes of a row, both arrays
+          static_assert(stage_bytes<L>() <= sizeof(float2) * 2 * LINES * LineGeom<float, L>::STRIDE,
+                        "row slots must fit in the line buffers");
+          if (threadIdx.x == 0) {
+               mbar_init(bar, 1);
+               mbar_fence_init();
+          }
+          __syncthreads();   // the barrier is initialised before anyone waits on it
+          if (threadIdx.x == 0) {
+               mbar_expect_tx(bar, LINES * RB);
+               const float2 *r0 = y + ((size_t)b * N + (size_t)k1b * rowstride) * 2;
+#pragma unroll
+               for (int r = 0; r < LINES; r++)
+                    bulk_load(stage + r * (RB + kPad), r0 + (size_t)r * rowstride * 2, RB, bar);
+          }
+          load_table<float>(tw, twline, L);
+          const bool ok = mbar_wait(bar, 0u);
+          const float4 *row = reinterpret_cast<const float4 *>(stage + c * (RB + kPad));
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               const float4 q = row[t + m * (L / 8)];
+               v[0][m] = make_float2(q.x, q.y);
+               v[1][m] = make_float2(q.z, q.w);
+          }
+          if (!ok) atomicOr(err, ERR_STAGE_TIMEOUT);
+          // k_rowpass's barrier after this call keeps the first pass's stores
+          // (the slots alias the line buffers) behind every thread's reads
      }
 };
 

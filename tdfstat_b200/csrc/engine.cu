@@ -329,7 +329,7 @@ struct tdf_engine {
      std::vector<GraphEntry> graphs;
      uint64_t graph_tick = 0;
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
-     bool row_bulk = true;     // split-form row pass fetches its rows by bulk copies (TDF_ROW_BULK=0: per thread)
+     bool row_bulk = true;     // row passes fetch their rows by bulk copies (TDF_ROW_BULK=0: per thread)
      // optional per-kernel event timing
      bool timing = false;
      tdf_kernel_times kt{};
@@ -844,15 +844,10 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
                         e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G,
                         e->cand_cap, boff};
      tev = e->timing ? timing_begin(e, st) : (size_t)-1;
-     if constexpr (std::is_same<T, float>::value) {
-          if (e->row_bulk) {
-               RowsYBulk src{Ln.Ybuf.as<float2>(), e->nfftf, t.N2,
-                             reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1)};
-               TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
-          } else {
-               RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
-               TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
-          }
+     if (e->row_bulk) {
+          RowsYBulk<T> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2,
+                           reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1)};
+          TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
      } else {
           RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
           TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));

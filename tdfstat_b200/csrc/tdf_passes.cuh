@@ -202,30 +202,32 @@ struct RowsY {
      }
 };
 
-// RowsY for the split form with the CTA's LINES rows brought in by bulk
-// copies: row r (N2 elements of 16 bytes, both arrays) goes to shared offset
-// r * (16*N2 + 64), so that the 8 rows a warp reads from at once fall on
-// alternate halves of the banks; the slots alias the line buffers, which the
-// first pass only writes after the barrier that follows the reads.  Thread
+// RowsY<T, 2> with the CTA's LINES rows brought in by bulk copies: row r
+// (N2 elements of 2 cx<T>, both arrays) goes to shared offset
+// r * (EB*N2 + 64), so that the 8 rows a warp reads from at once do not all
+// start on the same bank; the slots alias the line buffers, which the first
+// pass only writes after k_rowpass's barrier that follows the reads.  Thread
 // 0 issues the copies; everyone waits on one mbarrier (bounded: on time-out
 // ERR_STAGE_TIMEOUT is or-ed into *err).
+template <typename T>
 struct RowsYBulk {
-     const float2 *y;
+     const cx<T> *y;
      int N;            // N1*N2
      int rowstride;    // N2
      unsigned *err;
      unsigned bar_off = 0;   // byte offset of the barrier in dynamic shared memory (set by the launcher)
      static constexpr bool kBulk = true;
      static constexpr unsigned kPad = 64;
+     static constexpr unsigned EB = 2 * sizeof(cx<T>);   // bytes of an element, both arrays
 
      template <int L>
-     __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)LINES * (16 * L + kPad); }
+     __host__ __device__ static constexpr size_t stage_bytes() { return (size_t)LINES * (EB * L + kPad); }
 
      template <int L>
-     __device__ __forceinline__ void load_bulk(float2 (&v)[2][8], int b, int k1b, int c, int t, unsigned char *stage,
-                                               uint64_t *bar, float2 *tw, const float2 *twline) const {
-          constexpr unsigned RB = 16 * L;   // bytes of a row, both arrays
-          static_assert(stage_bytes<L>() <= sizeof(float2) * 2 * LINES * LineGeom<float, L>::STRIDE,
+     __device__ __forceinline__ void load_bulk(cx<T> (&v)[2][8], int b, int k1b, int c, int t, unsigned char *stage,
+                                               uint64_t *bar, cx<T> *tw, const cx<T> *twline) const {
+          constexpr unsigned RB = EB * L;   // bytes of a row
+          static_assert(stage_bytes<L>() <= sizeof(cx<T>) * 2 * LINES * LineGeom<T, L>::STRIDE,
                         "row slots must fit in the line buffers");
           if (threadIdx.x == 0) {
                mbar_init(bar, 1);
@@ -234,19 +236,25 @@ struct RowsYBulk {
           __syncthreads();   // the barrier is initialised before anyone waits on it
           if (threadIdx.x == 0) {
                mbar_expect_tx(bar, LINES * RB);
-               const float2 *r0 = y + ((size_t)b * N + (size_t)k1b * rowstride) * 2;
+               const cx<T> *r0 = y + ((size_t)b * N + (size_t)k1b * rowstride) * 2;
 #pragma unroll
                for (int r = 0; r < LINES; r++)
                     bulk_load(stage + r * (RB + kPad), r0 + (size_t)r * rowstride * 2, RB, bar);
           }
-          load_table<float>(tw, twline, L);
+          load_table<T>(tw, twline, L);
           const bool ok = mbar_wait(bar, 0u);
-          const float4 *row = reinterpret_cast<const float4 *>(stage + c * (RB + kPad));
+          const unsigned char *row = stage + c * (RB + kPad);
 #pragma unroll
           for (int m = 0; m < 8; m++) {
-               const float4 q = row[t + m * (L / 8)];
-               v[0][m] = make_float2(q.x, q.y);
-               v[1][m] = make_float2(q.z, q.w);
+               const int e = t + m * (L / 8);
+               if constexpr (sizeof(T) == 4) {
+                    const float4 q = reinterpret_cast<const float4 *>(row)[e];
+                    v[0][m] = make_float2(q.x, q.y);
+                    v[1][m] = make_float2(q.z, q.w);
+               } else {
+                    v[0][m] = reinterpret_cast<const cx<T> *>(row)[2 * e];
+                    v[1][m] = reinterpret_cast<const cx<T> *>(row)[2 * e + 1];
+               }
           }
           if (!ok) atomicOr(err, ERR_STAGE_TIMEOUT);
           // k_rowpass's barrier after this call keeps the first pass's stores

@@ -496,19 +496,20 @@ static int staged_setup(tdf_engine *e) {
      PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
      if (!encode) return TDF_OK;
      for (int k = 0; k < 2; k++) {
+          // interleaved operands: sample i, detector d at word (slot*Nal + i)*nifo + d
           const cuuint64_t rowsx = (cuuint64_t)(e->Nal / N2);
-          const cuuint64_t dx[4] = {(cuuint64_t)4 * N2, rowsx, (cuuint64_t)nifo, (cuuint64_t)e->Bs};
-          const cuuint64_t sx[3] = {(cuuint64_t)N2 * 16, (cuuint64_t)e->Nal * 16, (cuuint64_t)nifo * e->Nal * 16};
-          const cuuint32_t bx[4] = {4 * LINES, (cuuint32_t)R, (cuuint32_t)nifo, 1};
-          const cuuint64_t ds[4] = {(cuuint64_t)N2, rowsx, (cuuint64_t)nifo, (cuuint64_t)e->Bs};
-          const cuuint64_t ss[3] = {(cuuint64_t)N2 * 4, (cuuint64_t)e->Nal * 4, (cuuint64_t)nifo * e->Nal * 4};
-          const cuuint32_t bs[4] = {LINES, (cuuint32_t)R, (cuuint32_t)nifo, 1};
-          const cuuint32_t one[4] = {1, 1, 1, 1};
-          CUresult r = encode(&e->tm_x[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, e->xab[k].p, dx, sx, bx, one,
+          const cuuint64_t dx[3] = {(cuuint64_t)4 * nifo * N2, rowsx, (cuuint64_t)e->Bs};
+          const cuuint64_t sx[2] = {(cuuint64_t)nifo * N2 * 16, (cuuint64_t)e->Nal * nifo * 16};
+          const cuuint32_t bx[3] = {(cuuint32_t)(4 * nifo * LINES), (cuuint32_t)R, 1};
+          const cuuint64_t ds[3] = {(cuuint64_t)nifo * N2, rowsx, (cuuint64_t)e->Bs};
+          const cuuint64_t ss[2] = {(cuuint64_t)nifo * N2 * 4, (cuuint64_t)e->Nal * nifo * 4};
+          const cuuint32_t bs[3] = {(cuuint32_t)(nifo * LINES), (cuuint32_t)R, 1};
+          const cuuint32_t one[3] = {1, 1, 1};
+          CUresult r = encode(&e->tm_x[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, e->xab[k].p, dx, sx, bx, one,
                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
           if (r != CUDA_SUCCESS) return set_error(TDF_ERR_CUDA, "cuTensorMapEncodeTiled (operands xab): %d", (int)r);
-          r = encode(&e->tm_s[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, e->s2[k].p, ds, ss, bs, one,
+          r = encode(&e->tm_s[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, e->s2[k].p, ds, ss, bs, one,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
           if (r != CUDA_SUCCESS) return set_error(TDF_ERR_CUDA, "cuTensorMapEncodeTiled (operands s2): %d", (int)r);
@@ -830,7 +831,8 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
                pro.smem = e->stg_smem;
                TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
           } else {
-               DemodSplit pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal, e->nifo};
+               DemodSplitIL pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal,
+                                e->nifo};
                TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
           }
      } else {

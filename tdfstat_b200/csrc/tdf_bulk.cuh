@@ -59,6 +59,16 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
          : "memory");
 }
 
+// Tiled 3-D TMA load of one box into shared memory (no multicast); x as
+// for tma_load_4d.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+     asm volatile(
+         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+         "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+         : "memory");
+}
+
 // Tiled 4-D TMA load of one box into shared memory (no multicast).  The
 // innermost coordinate x times the element size must be a multiple of 16
 // bytes; callers only pass x that are multiples of 8 elements of 4 bytes.

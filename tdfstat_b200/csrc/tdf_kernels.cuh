@@ -103,9 +103,10 @@ __global__ void __launch_bounds__(256) k_sky_prep(
                                            __dmul_rn(S.nS2, e[3 * (size_t)i + 2]));
                const double sh1 = __dadd_rn(__dadd_rn(__dmul_rn(S.nS0, e[0]), __dmul_rn(S.nS1, e[1])), __dmul_rn(S.nS2, e[2]));
                shftf[(size_t)q * Nal + i] = __dsub_rn(sh, sh1);
-               const size_t o = ((size_t)p * nifo + d) * Nal + i;
+               const size_t o = ((size_t)p * nifo + d) * Nal + i;      // planar (FP64 operands)
+               const size_t oi = ((size_t)p * Nal + i) * nifo + d;     // interleaved by detector (split)
                const double di = (double)i;
-               if (s2) s2[o] = (float)__dmul_rn((double)(2 * i), sh);
+               if (s2) s2[oi] = (float)__dmul_rn((double)(2 * i), sh);
                if (t1) t1[o] = __dadd_rn(__dmul_rn(di, di), __dmul_rn((double)(2 * i), sh));
                const double phase = __dadd_rn(__dmul_rn(S.het0, di), __dmul_rn(oms, sh));
                double sn, cn;
@@ -249,7 +250,8 @@ __device__ __forceinline__ double2 splint_eval(const double2 *__restrict__ ya, c
 }
 
 // grid (ceil(N/256), Q), 256 threads: xDatm{a,b}[i] = splint(...)/sig2 as
-// split (float4 xa.re, xa.im, xb.re, xb.im) or FP64 (two double2) operands
+// split (float4 xa.re, xa.im, xb.re, xb.im, interleaved by detector:
+// [slot][i][det]) or FP64 (two double2, planar: [slot][det][i]) operands
 __global__ void __launch_bounds__(256) k_splint(
      const double2 *__restrict__ Z, const double2 *__restrict__ Y2, size_t stride,
      const double *__restrict__ shftf, int Nal, int N, int n, int interpftpad,
@@ -264,9 +266,12 @@ __global__ void __launch_bounds__(256) k_splint(
      const double2 vb = splint_eval(Z + ((size_t)q * 2 + 1) * stride, Y2 + ((size_t)q * 2 + 1) * stride, n, x);
      const double s2 = dp[d].sig2;
      const double2 a = make_double2(va.x / s2, va.y / s2), b = make_double2(vb.x / s2, vb.y / s2);
-     const size_t o = ((size_t)p * nifo + d) * Nal + i;
-     if (xab) xab[o] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
-     if (xa64) { xa64[o] = a; xb64[o] = b; }
+     if (xab) xab[((size_t)p * Nal + i) * nifo + d] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+     if (xa64) {
+          const size_t o = ((size_t)p * nifo + d) * Nal + i;
+          xa64[o] = a;
+          xb64[o] = b;
+     }
 }
 
 // ------------------------------------------------------------------ spindown stage
@@ -287,7 +292,8 @@ struct CompSum {
 // plus spnd*(2 i shft_n[i]) in FP32 per detector; FP32 sincos and products.
 // The detector-network sum is compensated (Neumaier) for three or more
 // detectors; for one or two it is a single rounded addition, which the
-// compensation would not change.
+// compensation would not change.  Operands planar by detector,
+// xab[(slot*nifo + d)*Nal + i] (the layout tdf_fstat_operands_static takes).
 struct DemodSplit {
      const float4 *xab;
      const float *s2;
@@ -387,18 +393,79 @@ struct DemodSplit {
      }
 };
 
-// DemodSplit with its operands brought in by TMA.  Thread (c, t) of the CTA
+// DemodSplit over operands interleaved by detector, xab[(slot*Nal + i)*nifo
+// + d] and s2 likewise (the engine's layout): with two detectors a sample's
+// operands are two adjacent 16-byte words and one 8-byte word, each read
+// from one address, and one pointer per operand array steps through the
+// thread's samples.  Same arithmetic, in the same order, as DemodSplit.
+struct DemodSplitIL {
+     const float4 *xab;
+     const float *s2;
+     const TmplParam *tp;
+     int N, N2, Nal, nifo;
+
+     template <int L>
+     __device__ __forceinline__ void load(float2 (&v)[2][8], int b, int n2, int t) const {
+          const TmplParam P = tp[b];
+          const float spf = (float)P.spnd;
+          const int i0 = N2 * t + n2;
+          const int di = N2 * (L / 8);    // samples between the thread's elements
+          const int de = di * nifo;       // operand words between them
+          const size_t e0 = ((size_t)P.slot * Nal + i0) * nifo;
+          const float4 *xp = xab + e0;
+          const float *sp = s2 + e0;
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               const int i = i0 + m * di;
+               float2 fa = make_float2(0.f, 0.f), fb = make_float2(0.f, 0.f);
+               if (i < N) {
+                    const double dd = (double)i;
+                    const double ph = fma(P.spnd, dd * dd, P.het1 * dd);
+                    const double kk = rint(ph * INV_TWO_PI);
+                    const float pr = (float)fma(-kk, TWO_PI, ph);
+                    const float4 *x = xp + m * de;
+                    const float *s = sp + m * de;
+                    if (nifo == 2) {
+                         const float2 ss = __ldg(reinterpret_cast<const float2 *>(s));
+                         DemodSplit::rot(__ldg(x), fmaf(spf, ss.x, pr), fa, fb);
+                         float2 pa, pb;
+                         DemodSplit::rot(__ldg(x + 1), fmaf(spf, ss.y, pr), pa, pb);
+                         fa = cadd(fa, pa);
+                         fb = cadd(fb, pb);
+                    } else if (nifo == 1) {
+                         DemodSplit::rot(__ldg(x), fmaf(spf, __ldg(s), pr), fa, fb);
+                    } else {
+                         CompSum ar, ai, br, bi;
+                         for (int d = 0; d < nifo; d++) {
+                              float2 pa, pb;
+                              DemodSplit::rot(__ldg(x + d), fmaf(spf, __ldg(s + d), pr), pa, pb);
+                              if (d == 0) { ar.init(pa.x); ai.init(pa.y); br.init(pb.x); bi.init(pb.y); }
+                              else { ar.add(pa.x); ai.add(pa.y); br.add(pb.x); bi.add(pb.y); }
+                         }
+                         fa = make_float2(ar.value(), ai.value());
+                         fb = make_float2(br.value(), bi.value());
+                    }
+               }
+               v[0][m] = fa;
+               v[1][m] = fb;
+          }
+     }
+};
+
+// DemodSplitIL with its operands brought in by TMA.  Thread (c, t) of the CTA
 // needs, for element m, the samples of row n1 = t + m*R (R = L/8) of column
 // n2 = x0 + c, so the rows of a group m of the CTA's LINES columns, every
-// detector, form one box of each operand tensor:
-//   xab as floats {4*N2, rows, nifo, slots}, box {4*LINES, R, nifo, 1}
-//   s2            {N2,   rows, nifo, slots}, box {LINES,   R, nifo, 1}
+// detector, form one box of each operand tensor (interleaved layout):
+//   xab as floats {4*nifo*N2, rows, slots}, box {4*nifo*LINES, R, 1}
+//   s2            {nifo*N2,   rows, slots}, box {nifo*LINES,   R, 1}
 // (rows = Nal/N2, Nal a multiple of N2).  The groups holding samples < N go
 // through a ring of `stages` shared-memory slots that aliases the line
 // buffers (unused until the first FFT pass stores), each slot completing on
 // its own mbarrier; all copies of the ring are in flight while the threads
 // demodulate, instead of one element's loads per thread at a time.
 // The arithmetic per element is DemodSplit's, in the same order.
+// Opt-in (TDF_STAGED_OPERANDS=1): with the operands L2-resident it measured
+// slower than DemodSplitIL's per-thread loads.
 struct DemodSplitStaged {
      CUtensorMap mx;    // xab
      CUtensorMap ms;    // s2
@@ -416,8 +483,8 @@ struct DemodSplitStaged {
                                            unsigned xbytes, int x0, int w) const {
           unsigned char *dst = ring + (size_t)s * slot_bytes;
           mbar_expect_tx(&bars[s], slot_bytes);
-          tma_load_4d(dst, &mx, 4 * x0, g * (L / 8), 0, w, &bars[s]);
-          tma_load_4d(dst + xbytes, &ms, x0, g * (L / 8), 0, w, &bars[s]);
+          tma_load_3d(dst, &mx, 4 * nifo * x0, g * (L / 8), w, &bars[s]);
+          tma_load_3d(dst + xbytes, &ms, nifo * x0, g * (L / 8), w, &bars[s]);
      }
 
      template <int L>
@@ -454,11 +521,11 @@ struct DemodSplitStaged {
                          const double ph = fma(P.spnd, di * di, P.het1 * di);
                          const double kk = rint(ph * INV_TWO_PI);
                          const float pr = (float)fma(-kk, TWO_PI, ph);
-                         const int e0 = t * LINES + c;
+                         const int e0 = (t * LINES + c) * nifo;
                          if (nifo <= 2) {
                               DemodSplit::rot(X[e0], fmaf(spf, S2[e0], pr), fa, fb);
                               if (nifo == 2) {
-                                   const int e1 = (R + t) * LINES + c;
+                                   const int e1 = e0 + 1;
                                    float2 pa, pb;
                                    DemodSplit::rot(X[e1], fmaf(spf, S2[e1], pr), pa, pb);
                                    fa = cadd(fa, pa);
@@ -467,7 +534,7 @@ struct DemodSplitStaged {
                          } else {
                               CompSum ar, ai, br, bi;
                               for (int d = 0; d < nifo; d++) {
-                                   const int ed = (d * R + t) * LINES + c;
+                                   const int ed = e0 + d;
                                    float2 pa, pb;
                                    DemodSplit::rot(X[ed], fmaf(spf, S2[ed], pr), pa, pb);
                                    if (d == 0) { ar.init(pa.x); ai.init(pa.y); br.init(pb.x); bi.init(pb.y); }

@@ -59,3 +59,19 @@ def test_records_do_not_depend_on_chunk_size(golden):
         with pytest.raises(TdfError):
             eng.templates_per_chunk = bad
     eng.close()
+
+
+@pytest.mark.parametrize("name", ["g2_h1l1_inj", "g1_h1_directed"])
+def test_tma_staged_operands_match(golden, monkeypatch, name):
+    """TDF_STAGED_OPERANDS=1 (column-pass operands brought in by TMA boxes)
+    computes the same arithmetic as the default per-thread loads."""
+    from tdfstat_b200.engine import Engine
+    g = golden(name)
+    pm, mm, nn = g.job32.sky_points()
+    eng = Engine.from_job(g.job32, form="split")
+    ref = _records(eng.search(pm, mm, nn))
+    eng.close()
+    monkeypatch.setenv("TDF_STAGED_OPERANDS", "1")
+    eng = Engine.from_job(g.job32, form="split")
+    _same(_records(eng.search(pm, mm, nn)), ref)
+    eng.close()

@@ -166,6 +166,34 @@ int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const f
 int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss,
                        double *F, int64_t nF);
 
+/* A continuous-wave signal to inject: the fields of the reference's signal
+   file (read_signal_file, init.c:300-358) and the settings add_signal()
+   reads (init.c:365-504). */
+typedef struct tdf_signal {
+     double h0;                /* GW amplitude (the 'amp' form); used when snr <= 0 */
+     double snr;               /* > 0: h0 = snr / sqrt(sum_n sum_i s_n[i]^2 / sig2_n) */
+     double freq, fdot;        /* [Hz], [Hz/s] in the reference segment */
+     double ra, dec;           /* [rad] */
+     double iota, psi, phase;  /* [rad] */
+     double fpo, B;            /* band start and width [Hz] (sett->fpo, sett->B) */
+     int32_t reffr;            /* reference segment of freq */
+     int32_t seg;              /* this segment's number (opts->seg) */
+} tdf_signal;
+
+/* add_signal() (init.c:365-504) on the engine's resident data, replacing
+   the host-side call main.c:101-104 makes before the search: h0*s_n[i] is
+   added to detector n's xDat[i] wherever xDat[i] != 0; sig2 keeps the value
+   of the data as read.  A signal outside [fpo, fpo + B] adds nothing
+   (*in_band = 0), as in the reference.  *h0 (may be NULL) receives the
+   amplitude used.  The reference's 'snr' form reads sig2 past the detector
+   array (init.c:462-464); snr > 0 here is the network SNR above instead.
+   tdf_engine_upload() replaces the data, injection included. */
+int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0, int32_t *in_band);
+
+/* Copies detector det's resident xDat (the first n <= N floats, injections
+   included) to the host. */
+int tdf_engine_get_xdat(tdf_engine *e, int32_t det, float *xdat, int64_t n);
+
 /* F-statistic of one template of the split form from spindown operands that
    are already on the device, without allocating any memory.  No counterpart
    in the reference: it is for callers that must not allocate device memory

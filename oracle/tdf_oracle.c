@@ -57,6 +57,63 @@ void orc_modvir(const tdf_segment *seg, int det, double sinal, double cosal,
      }
 }
 
+/* search/network/openmp/init.c:365-504 (add_signal), 'amp' form, with the
+   'snr' form as the network SNR (the reference's reads sig2 of ifo[nifo],
+   init.c:462-464).  Expressions in the reference's evaluation order. */
+int orc_add_signal(const tdf_segment *seg, const tdf_signal *sig, double *h0_out)
+{
+     const int N = seg->N, nifo = seg->nifo;
+     const int dseg = sig->seg - sig->reffr;
+     double freqo0 = 2 * M_PI * sig->freq * seg->dt;
+     const double freqo1 = M_PI * sig->fdot * seg->dt * seg->dt;
+     freqo0 += 2. * freqo1 * (seg->N) * dseg;                              /* init.c:386 */
+     if (freqo0 / (2 * M_PI * seg->dt) < sig->fpo || freqo0 / (2 * M_PI * seg->dt) > sig->fpo + sig->B)
+          return 1;                                                         /* init.c:389-395 */
+     const double sinalpha = sin(sig->ra), cosalpha = cos(sig->ra);
+     const double sindelta = sin(sig->dec), cosdelta = cos(sig->dec);
+     const double cosi = cos(sig->iota), psi = sig->psi, phi = sig->phase;
+     const double cosip = (1. + cosi * cosi) / 2.;
+     double amplit[4];                                                      /* init.c:411-414 */
+     amplit[0] = cos(2. * psi) * cosip * cos(phi) - sin(2. * psi) * cosi * sin(phi);
+     amplit[1] = sin(2. * psi) * cosip * cos(phi) + cos(2. * psi) * cosi * sin(phi);
+     amplit[2] = -cos(2. * psi) * cosip * sin(phi) - sin(2. * psi) * cosi * cos(phi);
+     amplit[3] = -sin(2. * psi) * cosip * sin(phi) + cos(2. * psi) * cosi * cos(phi);
+     const double phaseshift = freqo0 * seg->N * dseg - freqo1 * pow(seg->N * dseg, 2);   /* init.c:417-418 */
+     double *s = (double *)malloc((size_t)nifo * N * sizeof(double));
+     double *aa = (double *)malloc((size_t)N * sizeof(double));
+     double *bb = (double *)malloc((size_t)N * sizeof(double));
+     double net = 0.;
+     for (int n = 0; n < nifo; n++) {
+          const tdf_detector *d = &seg->det[n];
+          orc_modvir(seg, n, sinalpha, cosalpha, sindelta, cosdelta, aa, bb);
+          const double nSource[3] = {cosalpha * cosdelta, sinalpha * cosdelta, sindelta};
+          double sum = 0.;
+          for (int i = 0; i < N; i++) {
+               double shiftadd = 0.;
+               for (int j = 0; j < 3; j++) shiftadd += nSource[j] * d->detssb[i * 3 + j];
+               double phaseadd = freqo0 * (i + shiftadd) +
+                                 freqo1 * (2. * shiftadd * i + SQR((double)i) + shiftadd * shiftadd) + phaseshift;
+               phaseadd -= 2 * M_PI * seg->dt * sig->fpo * i;                 /* init.c:444-447 */
+               const double v = amplit[0] * (aa[i]) * cos(phaseadd) + amplit[1] * (bb[i]) * cos(phaseadd) +
+                                amplit[2] * (aa[i]) * sin(phaseadd) + amplit[3] * (bb[i]) * sin(phaseadd);
+               s[(size_t)n * N + i] = v;
+               sum += v * v;
+          }
+          net += sum / d->sig2;
+     }
+     const double h0 = sig->snr > 0. ? sig->snr / sqrt(net) : sig->h0;
+     for (int n = 0; n < nifo; n++) {
+          float *x = (float *)seg->det[n].xdat;
+          for (int i = 0; i < N; i++)
+               if (x[i]) x[i] += h0 * s[(size_t)n * N + i];                   /* init.c:468-473 */
+     }
+     free(s);
+     free(aa);
+     free(bb);
+     if (h0_out) *h0_out = h0;
+     return 0;
+}
+
 /* search/network/openmp/auxi.c:93-117 (natural cubic spline, unit spacing).
    The forward-sweep factors are real: y2[i] = -0.5*invp, invp = 2/(y2[i-1]+4). */
 static void orc_spline(const double complex *y, int n, double complex *y2)

@@ -47,6 +47,13 @@ void orc_modvir(const tdf_segment *seg, int det, double sinal, double cosal,
 void orc_splintpad(const double complex *ya, const double *shftf, int N,
                    int interpftpad, double complex *out);
 
+/* add_signal (init.c:365-504): adds h0*s_n[i] to seg->det[n].xdat[i] where
+   it is nonzero, in place (the xdat arrays must be the caller's writable
+   copies).  sig->snr > 0 sets h0 from the network SNR (tdf_signal).
+   Returns 1 if the signal lies outside [fpo, fpo + B] (nothing added),
+   else 0; *h0 receives the amplitude used. */
+int orc_add_signal(const tdf_segment *seg, const tdf_signal *sig, double *h0);
+
 /* textbook FFT (fft_core.c), exposed for the FFT tests */
 int orc_fft(int n, int sign, const double complex *in, double complex *out);
 

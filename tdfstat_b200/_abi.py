@@ -86,6 +86,24 @@ class TdfRecord(C.Structure):
     ]
 
 
+class TdfSignal(C.Structure):
+    _fields_ = [
+        ("h0", C.c_double),
+        ("snr", C.c_double),
+        ("freq", C.c_double),
+        ("fdot", C.c_double),
+        ("ra", C.c_double),
+        ("dec", C.c_double),
+        ("iota", C.c_double),
+        ("psi", C.c_double),
+        ("phase", C.c_double),
+        ("fpo", C.c_double),
+        ("B", C.c_double),
+        ("reffr", C.c_int32),
+        ("seg", C.c_int32),
+    ]
+
+
 class TdfKernelTimes(C.Structure):
     _fields_ = [
         ("colpass_ms", C.c_double),
@@ -124,6 +142,8 @@ ABI_FUNCTIONS = [
      [P, C.c_int, I32P, F32P, F32P, F32P, I64P, I64P]),
     ("tdf_fstat_spectrum", C.c_int,
      [P, C.c_int32, C.c_float, C.c_float, C.c_float, F64P, C.c_int64]),
+    ("tdf_engine_add_signal", C.c_int, [P, C.POINTER(TdfSignal), F64P, I32P]),
+    ("tdf_engine_get_xdat", C.c_int, [P, C.c_int32, F32P, C.c_int64]),
     ("tdf_fstat_operands_static", C.c_int,
      [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_float, C.c_float,
       C.c_int32, C.c_int32, P, P]),

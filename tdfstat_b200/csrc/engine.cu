@@ -1440,6 +1440,81 @@ int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const f
      return TDF_OK;
 }
 
+// add_signal (init.c:365-504) on the resident xDat.  The constants are
+// formed here as the reference forms them; k_signal computes s_n[i] into the
+// sky-stage scratch B0 (idle between searches), k_add_signal adds h0 s_n[i].
+int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0_out, int32_t *in_band) {
+     if (!e || !sig) return set_error(TDF_ERR_INVALID, "null engine or signal");
+     if (in_band) *in_band = 0;
+     CUCHK(cudaSetDevice(e->dev));
+     const int N = e->N, nifo = e->nifo;
+     const double dt = e->seg.dt;
+     const int dseg = sig->seg - sig->reffr;
+     double freqo0 = 2 * M_PI * sig->freq * dt;
+     const double freqo1 = M_PI * sig->fdot * dt * dt;
+     freqo0 += 2. * freqo1 * N * dseg;
+     if (freqo0 / (2 * M_PI * dt) < sig->fpo || freqo0 / (2 * M_PI * dt) > sig->fpo + sig->B) return TDF_OK;
+     SignalParam P;
+     P.sinal = std::sin(sig->ra);
+     P.cosal = std::cos(sig->ra);
+     P.sindel = std::sin(sig->dec);
+     P.cosdel = std::cos(sig->dec);
+     const double cosi = std::cos(sig->iota), psi = sig->psi, phi = sig->phase;
+     const double cosip = (1. + cosi * cosi) / 2.;
+     P.amp[0] = std::cos(2. * psi) * cosip * std::cos(phi) - std::sin(2. * psi) * cosi * std::sin(phi);
+     P.amp[1] = std::sin(2. * psi) * cosip * std::cos(phi) + std::cos(2. * psi) * cosi * std::sin(phi);
+     P.amp[2] = -std::cos(2. * psi) * cosip * std::sin(phi) - std::sin(2. * psi) * cosi * std::cos(phi);
+     P.amp[3] = -std::sin(2. * psi) * cosip * std::sin(phi) + std::cos(2. * psi) * cosi * std::cos(phi);
+     P.nS0 = P.cosal * P.cosdel;
+     P.nS1 = P.sinal * P.cosdel;
+     P.nS2 = P.sindel;
+     P.freqo0 = freqo0;
+     P.freqo1 = freqo1;
+     P.phaseshift = freqo0 * N * dseg - freqo1 * std::pow((double)(N * dseg), 2);
+     P.dephase = 2 * M_PI * dt * sig->fpo;
+     const int nblk = (N + 255) / 256;
+     if (e->B0.bytes < (size_t)nifo * N * sizeof(double) || e->partial.bytes < (size_t)nifo * nblk * sizeof(double))
+          return set_error(TDF_ERR_UNSUPPORTED, "injection scratch too small");
+     CUCHK(cudaStreamSynchronize(e->sky_stream));
+     cudaStream_t st = e->stream;
+     double *s = e->B0.as<double>();
+     double *part = e->partial.as<double>();
+     k_signal<<<dim3(nblk, nifo), 256, 0, st>>>(e->xdat.as<float>(), e->detssb.as<double>(), e->cosm.as<double>(),
+                                                e->sinm.as<double>(), e->detp.as<DetParam>(), N, e->Nal, P, s, part);
+     CUCHK(cudaGetLastError());
+     double h0 = sig->h0;
+     if (sig->snr > 0.) {
+          std::vector<double> ps((size_t)nifo * nblk);
+          CUCHK(cudaMemcpyAsync(ps.data(), part, ps.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+          CUCHK(cudaStreamSynchronize(st));
+          double net = 0.;
+          for (int n = 0; n < nifo; n++) {
+               double sum = 0.;
+               for (int b = 0; b < nblk; b++) sum += ps[(size_t)n * nblk + b];
+               net += sum / e->dets[n].sig2;
+          }
+          if (!(net > 0.)) return set_error(TDF_ERR_INVALID, "signal has no power in the data (snr form)");
+          h0 = sig->snr / std::sqrt(net);
+     }
+     k_add_signal<<<dim3(nblk, nifo), 256, 0, st>>>(e->xdat.as<float>(), s, N, e->Nal, h0);
+     CUCHK(cudaGetLastError());
+     CUCHK(cudaStreamSynchronize(st));
+     e->launches += 2;
+     if (h0_out) *h0_out = h0;
+     if (in_band) *in_band = 1;
+     return TDF_OK;
+}
+
+int tdf_engine_get_xdat(tdf_engine *e, int32_t det, float *xdat, int64_t n) {
+     if (!e || !xdat) return set_error(TDF_ERR_INVALID, "null argument");
+     if (det < 0 || det >= e->nifo || n < 0 || n > e->N)
+          return set_error(TDF_ERR_INVALID, "detector %d of %d, %lld samples of %d", det, e->nifo, (long long)n, e->N);
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     CUCHK(cudaMemcpy(xdat, e->xdat.as<float>() + (size_t)det * e->Nal, n * sizeof(float), cudaMemcpyDeviceToHost));
+     return TDF_OK;
+}
+
 int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, double *F, int64_t nF) {
      if (!e || !F) return set_error(TDF_ERR_INVALID, "null engine or output");
      if (nF < e->nF) return set_error(TDF_ERR_CAPACITY, "need %d values", e->nF);

@@ -65,6 +65,27 @@ constexpr double M_PI_D = 3.14159265358979323846;
 
 // ------------------------------------------------------------------ sky stage
 
+// modvir (settings.c:254-294) at one sample: the amplitude modulations
+// a(t), b(t) of detector D for a source at (alpha, delta), 0 where
+// |xDat[t]| <= DBL_MIN
+__device__ __forceinline__ void modvir_at(const DetParam &D, double sinal, double cosal, double sindel, double cosdel,
+                                          double cosm, double sinm, float x, double &aa, double &bb) {
+     aa = 0.;
+     bb = 0.;
+     if (fabs((double)x) > DBL_MIN) {
+          const double cosalfr = cosal * D.cphir + sinal * D.sphir;
+          const double sinalfr = sinal * D.cphir - cosal * D.sphir;
+          const double c2d = cosdel * cosdel, c2sd = sindel * cosdel;
+          const double c = cosalfr * cosm + sinalfr * sinm;
+          const double s = sinalfr * cosm - cosalfr * sinm;
+          const double c2s = 2. * c * c, cs = c * s;
+          aa = D.amod[0] * (2. - c2d) * c2s + D.amod[1] * (2. - c2d) * 2. * cs +
+               D.amod[2] * c2sd * c + D.amod[3] * c2sd * s - D.amod[0] * (2. - c2d) + D.amod[4] * c2d;
+          bb = D.amod[5] * sindel * c2s + D.amod[6] * sindel * 2. * cs +
+               D.amod[7] * cosdel * c + D.amod[8] * cosdel * s - D.amod[5] * sindel;
+     }
+}
+
 // grid (ceil(nfft/256), Q = npts*nifo), 256 threads
 __global__ void __launch_bounds__(256) k_sky_prep(
      const float *__restrict__ xdat, const double *__restrict__ detssb,
@@ -83,19 +104,8 @@ __global__ void __launch_bounds__(256) k_sky_prep(
                const SkyParam S = sp[p];
                const DetParam &D = dp[d];
                const float x = xdat[(size_t)d * Nal + i];
-               double aa = 0., bb = 0.;
-               if (fabs((double)x) > DBL_MIN) {
-                    const double cosalfr = S.cosalt * D.cphir + S.sinalt * D.sphir;
-                    const double sinalfr = S.sinalt * D.cphir - S.cosalt * D.sphir;
-                    const double c2d = S.cosdelt * S.cosdelt, c2sd = S.sindelt * S.cosdelt;
-                    const double c = cosalfr * cosm[i] + sinalfr * sinm[i];
-                    const double s = sinalfr * cosm[i] - cosalfr * sinm[i];
-                    const double c2s = 2. * c * c, cs = c * s;
-                    aa = D.amod[0] * (2. - c2d) * c2s + D.amod[1] * (2. - c2d) * 2. * cs +
-                         D.amod[2] * c2sd * c + D.amod[3] * c2sd * s - D.amod[0] * (2. - c2d) + D.amod[4] * c2d;
-                    bb = D.amod[5] * S.sindelt * c2s + D.amod[6] * S.sindelt * 2. * cs +
-                         D.amod[7] * S.cosdelt * c + D.amod[8] * S.cosdelt * s - D.amod[5] * S.sindelt;
-               }
+               double aa, bb;
+               modvir_at(D, S.sinalt, S.cosalt, S.sindelt, S.cosdelt, cosm[i], sinm[i], x, aa, bb);
                const double *e = detssb + (size_t)d * 3 * N;
                // shift and phase without FMA contraction: the phase reaches
                // ~1e5 rad, so its rounding must follow the reference's
@@ -136,6 +146,73 @@ __global__ void __launch_bounds__(256) k_sky_prep(
           partial[((size_t)q * gridDim.x + blockIdx.x) * 2 + 0] = sa;
           partial[((size_t)q * gridDim.x + blockIdx.x) * 2 + 1] = sb;
      }
+}
+
+// ------------------------------------------------------------------ injection
+
+// add_signal (init.c:365-504) constants, formed on the host in the
+// reference's evaluation order
+struct SignalParam {
+     double sinal, cosal, sindel, cosdel;   // of the source
+     double nS0, nS1, nS2;                  // cos a cos d, sin a cos d, sin d
+     double amp[4];                         // amplit[] (init.c:411-414)
+     double freqo0, freqo1, phaseshift;     // init.c:382-386, 417-418
+     double dephase;                        // 2 pi dt fpo (init.c:447)
+};
+
+// grid (ceil(N/256), nifo), 256 threads: the signal s_n[i] of detector n
+// (init.c:428-456) into s[n*N + i], and per-block sums of s^2 into
+// partial[n*gridDim.x + block].  Products and sums are not contracted, as
+// in the reference's DOUBLE build (the phase reaches ~1e8 rad).
+__global__ void __launch_bounds__(256) k_signal(
+     const float *__restrict__ xdat, const double *__restrict__ detssb, const double *__restrict__ cosm,
+     const double *__restrict__ sinm, const DetParam *__restrict__ dp, int N, int Nal, SignalParam P,
+     double *__restrict__ s, double *__restrict__ partial)
+{
+     const int d = blockIdx.y;
+     const int i = blockIdx.x * 256 + threadIdx.x;
+     double v = 0.;
+     if (i < N) {
+          const DetParam &D = dp[d];
+          double aa, bb;
+          modvir_at(D, P.sinal, P.cosal, P.sindel, P.cosdel, cosm[i], sinm[i], xdat[(size_t)d * Nal + i], aa, bb);
+          const double *e = detssb + (size_t)d * 3 * N + 3 * (size_t)i;
+          const double sh = __dadd_rn(__dadd_rn(__dmul_rn(P.nS0, e[0]), __dmul_rn(P.nS1, e[1])), __dmul_rn(P.nS2, e[2]));
+          const double di = (double)i;
+          // freqo0*(i + sh) + freqo1*(2 sh i + i^2 + sh^2) + phaseshift - dephase*i
+          const double q = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(2., sh), di), __dmul_rn(di, di)), __dmul_rn(sh, sh));
+          double ph = __dadd_rn(__dadd_rn(__dmul_rn(P.freqo0, __dadd_rn(di, sh)), __dmul_rn(P.freqo1, q)), P.phaseshift);
+          ph = __dsub_rn(ph, __dmul_rn(P.dephase, di));
+          double sn, cn;
+          sincos(ph, &sn, &cn);
+          v = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(P.amp[0], aa), cn), __dmul_rn(__dmul_rn(P.amp[1], bb), cn)),
+                                  __dmul_rn(__dmul_rn(P.amp[2], aa), sn)),
+                        __dmul_rn(__dmul_rn(P.amp[3], bb), sn));
+          s[(size_t)d * N + i] = v;
+     }
+     double v2 = v * v;
+#pragma unroll
+     for (int o = 16; o > 0; o >>= 1) v2 += __shfl_down_sync(0xffffffffu, v2, o);
+     __shared__ double red[8];
+     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v2;
+     __syncthreads();
+     if (threadIdx.x == 0) {
+          double t = 0.;
+          for (int k = 0; k < 8; k++) t += red[k];
+          partial[(size_t)d * gridDim.x + blockIdx.x] = t;
+     }
+}
+
+// grid (ceil(N/256), nifo), 256 threads: xDat[i] += h0 s_n[i] where xDat[i]
+// != 0, the sum in FP64 and rounded to float once (init.c:468-473)
+__global__ void __launch_bounds__(256) k_add_signal(float *__restrict__ xdat, const double *__restrict__ s, int N,
+                                                    int Nal, double h0)
+{
+     const int d = blockIdx.y;
+     const int i = blockIdx.x * 256 + threadIdx.x;
+     if (i >= N) return;
+     float *x = xdat + (size_t)d * Nal + i;
+     if (*x != 0.f) *x = (float)__dadd_rn((double)*x, __dmul_rn(h0, s[(size_t)d * N + i]));
 }
 
 // one CTA per sky point: aa = sum_n sum_i aa_n^2/sig2_n (jobcore.c:373-386);

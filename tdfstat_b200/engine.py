@@ -164,6 +164,19 @@ class Engine:
         _check(self.lib, st)
         return F
 
+    def add_signal(self, sig: _abi.TdfSignal) -> Tuple[float, bool]:
+        """Injects a CW signal into the resident data (add_signal, init.c:365-504);
+        returns (h0 used, whether the signal was in band)."""
+        h0, inb = C.c_double(0.0), C.c_int32(0)
+        _check(self.lib, self.lib.tdf_engine_add_signal(self.h, C.byref(sig), C.byref(h0), C.byref(inb)))
+        return h0.value, bool(inb.value)
+
+    def xdat(self, det: int, n: int) -> np.ndarray:
+        """The resident xDat of detector `det` (first n samples)."""
+        x = np.zeros(n, dtype=np.float32)
+        _check(self.lib, self.lib.tdf_engine_get_xdat(self.h, int(det), _p(x, C.c_float), n))
+        return x
+
     def stream(self) -> int:
         s = C.c_void_p()
         _check(self.lib, self.lib.tdf_engine_get_stream(self.h, C.byref(s)))

@@ -517,9 +517,31 @@ def read_band_vlines(path: str) -> List[List[float]]:
 
 # ---------------------------------------------------------------- the job
 
+def read_signal_file(path: str) -> Dict[str, float]:
+    """read_signal_file (init.c:300-358): skips tokens up to 'amp' or 'snr',
+    then reads h0 (or snr), reffr, freq, fdot, ra, dec, iota, psi, phase."""
+    with open(path) as f:
+        tok = f.read().split()
+    k = 0
+    while k < len(tok) and tok[k] not in ("amp", "snr"):
+        k += 1
+    if k == len(tok):
+        raise ValueError("%s: no 'amp' or 'snr' line" % path)
+    form = tok[k]
+    v = tok[k + 1:k + 10]
+    out = {"form": form, "reffr": int(v[1])}
+    out["h0" if form == "amp" else "snr"] = float(v[0])
+    for name, s in zip(("freq", "fdot", "ra", "dec", "iota", "psi", "phase"), v[2:]):
+        out[name] = float(s)
+    return out
+
+
 class Job:
     """Everything the reference's main() prepares before search(), built from
-    an INI file (main.c:33-116), plus the descriptors of include/tdfcuda.h."""
+    an INI file (main.c:33-116), plus the descriptors of include/tdfcuda.h.
+    A signal file named by search:addsig is read (job.signal, a tdf_signal)
+    but not applied: the engine applies it on the device
+    (Engine.add_signal), as main.c:101-104 does on the host."""
 
     def __init__(self, ini_path: str, float_build: bool = True):
         self.ini_path = ini_path
@@ -592,6 +614,19 @@ class Job:
         self.cosmodf, self.sinmodf = aux_arrays(N, self.sett.omr)
         self.range = set_search_range(self.sett, ini, float_build=float_build)
         self.sett.bufsize = self.sett.nfftf // 16 if self.gtype == "allsky" else self.sett.nfftf
+        self.signal = None
+        addsig = ini.get("search:addsig", "")
+        if addsig:
+            p = addsig if os.path.isabs(addsig) else os.path.join(base, addsig)
+            sp = read_signal_file(p)
+            sig = _abi.TdfSignal()
+            sig.h0 = sp.get("h0", 0.0)
+            sig.snr = sp.get("snr", 0.0)
+            for name in ("freq", "fdot", "ra", "dec", "iota", "psi", "phase"):
+                setattr(sig, name, sp[name])
+            sig.fpo, sig.B = self.sett.fpo, self.sett.B
+            sig.reffr, sig.seg = sp["reffr"], self.seg
+            self.signal = sig
         self._keep = []
 
     # descriptors ---------------------------------------------------------

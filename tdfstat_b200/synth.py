@@ -82,6 +82,7 @@ class Case:
     veto_flag: int = 0
     vlines_hz: Sequence[Sequence[float]] = ()   # veto intervals [Hz]
     injections: Sequence[Injection] = ()
+    addsig: Optional[Injection] = None          # written as the reference's signal file, not applied
     label: str = ""
 
     def settings(self) -> host.Settings:
@@ -274,7 +275,7 @@ def write_case(root: str, case: Case) -> str:
         "fstat_norm = %s" % case.fstat_norm,
         "grid_file = grid.bin",
         "usedet = %s" % "".join(case.dets),
-        "addsig = ",
+        "addsig = %s" % (os.path.join(root, "in", "signal.txt") if case.addsig else ""),
         "mods = %s" % ("read_O3" if case.read_o3 else ""),
         "label = %s" % case.label,
         "veto_flag = %d" % case.veto_flag,
@@ -287,6 +288,12 @@ def write_case(root: str, case: Case) -> str:
         "gsteps = %d %.9g %.9g %.9g" % tuple(case.gsteps),
         "",
     ]
+    if case.addsig:
+        # the reference's signal file (read_signal_file, init.c:300-358), 'amp' form
+        s = case.addsig
+        with open(os.path.join(indir, "signal.txt"), "w") as f:
+            f.write("amp %.17g %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n"
+                    % (s.h0, s.reffr, s.f, s.fdot, s.ra, s.dec, s.iota, s.psi, s.phase))
     ini = os.path.join(root, "search.ini")
     with open(ini, "w") as f:
         f.write("\n".join(lines))

@@ -29,6 +29,16 @@ CASES = {
         narrowdown=0.45, veto_flag=1, vlines_hz=((100.010, 100.0105), (100.0400, 100.0412)),
         injections=(synth.Injection(f=100.031, fdot=-4e-10, ra=2.1, dec=-0.4, iota=0.7, psi=0.3,
                                     phase=1.1, snr=40.0),)),
+    # the signal comes from a signal file (search:addsig) that the reference
+    # injects itself with add_signal() before its search; the data files hold
+    # noise only
+    "g4_addsig": synth.Case(
+        dt=8.0, nod=1, band=1440, dets=("H1", "L1"), sigma=(1.0, 1.2), seed=44, thr=8.0,
+        fdot_step=2e-10, sky_cells=12.0,
+        gtype="allsky_range", gcenter=(100.0412, -2e-10, 2.1, -0.4),
+        gsizes=(3600, 5.0, 1.0, 1.0), gsteps=(1, 1.0, 1.0, 1.0),
+        addsig=synth.Injection(f=100.0412, fdot=-2e-10, ra=2.1, dec=-0.4, iota=0.5, psi=0.8,
+                               phase=0.3, h0=0.3)),
     # all-sky grid (spindown range from Smin/Smax per sky point, both
     # hemispheres) with blocks_avg F-statistic normalisation
     "g3_allsky_blocks": synth.Case(

@@ -151,7 +151,39 @@ def load_oracle():
     lib.orc_fft.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     lib.orc_splintpad.restype = None
     lib.orc_splintpad.argtypes = [C.c_void_p, _abi.F64P, C.c_int, C.c_int, C.c_void_p]
+    lib.orc_add_signal.restype = C.c_int
+    lib.orc_add_signal.argtypes = [C.c_void_p, C.POINTER(_abi.TdfSignal), C.POINTER(C.c_double)]
     return lib
+
+
+class OracleSegment:
+    """job.segment() for the oracle, with the job's signal file (if any)
+    injected by orc_add_signal into copies of the xDat arrays, as the
+    reference's main() does before its search (main.c:101-104).  Keep the
+    object alive while the segment is used."""
+
+    def __init__(self, job, oracle):
+        self.seg = job.segment()
+        self.h0 = None
+        self.xdat = []
+        if job.signal is not None:
+            for n in range(self.seg.nifo):
+                x = np.array(job.dets[n].xdat, dtype=np.float32, copy=True)
+                self.xdat.append(x)
+                self.seg.det[n].xdat = x.ctypes.data_as(C.POINTER(C.c_float))
+            h0 = C.c_double(0.0)
+            assert oracle.orc_add_signal(C.byref(self.seg), C.byref(job.signal), C.byref(h0)) == 0
+            self.h0 = h0.value
+
+
+def engine_for(job, form="split", **kw):
+    """Engine.from_job plus the job's signal injected on the device."""
+    from tdfstat_b200.engine import Engine
+    eng = Engine.from_job(job, form=form, **kw)
+    if job.signal is not None:
+        h0, inband = eng.add_signal(job.signal)
+        assert inband
+    return eng
 
 
 def _ptr(a, t):

@@ -30,9 +30,17 @@ def test_dropin_matches_reference(golden, name, form):
     assert len(recs) == len(ref)
     np.testing.assert_array_equal(recs.pm, ref.pm)
     np.testing.assert_array_equal(recs.hdr[:, :3], ref.hdr[:, :3])
-    r = refkit.compare_records(recs, ref, f_rtol=2e-6 if form == "split" else 1e-12, F_rtol=TOL[form],
-                               thr=g.case.thr, tie_band=TOL[form])
+    tol = TOL[form]
+    if g.case.addsig is not None and form == "fp64":
+        # the drop-in host is the reference's default FLOAT build (-O3
+        # -ffast-math): its own add_signal() rounds the injected xDat
+        # differently from the DOUBLE build that made the fixture (~1e-7 in
+        # F); the library's FP64 path is checked at 1e-10 on the same
+        # injection by test_gpu_parity
+        tol = 1e-6
+    r = refkit.compare_records(recs, ref, f_rtol=2e-6 if form == "split" else 1e-12, F_rtol=tol,
+                               thr=g.case.thr, tie_band=tol)
     assert not r["unmatched"], r["unmatched"][:5]
-    assert r["max_F_rel"] <= TOL[form]
+    assert r["max_F_rel"] <= tol
     assert meta["totsgnl"] == recs.ntrig
     assert ">>" in out   # the reference's per-sky-point line

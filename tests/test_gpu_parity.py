@@ -21,8 +21,8 @@ TOL = {"fp64": 1e-10, "split": 1e-4}
 
 
 def _engine(job, form, **kw):
-    from tdfstat_b200.engine import Engine
-    return Engine.from_job(job, form=form, **kw)
+    # the case's signal file (g4) injected on the device, as main.c does on the host
+    return refkit.engine_for(job, form=form, **kw)
 
 
 def _match(rec, ref, form, thr):
@@ -67,7 +67,8 @@ def test_fstat_spectrum_matches_oracle(golden, oracle, name, form):
     import ctypes as C
     g = golden(name)
     job = g.job
-    seg, opts = job.segment(), job.search_opts()
+    os_ = refkit.OracleSegment(job, oracle)
+    seg, opts = os_.seg, job.search_opts()
     pm, mm, nn = job.sky_points()
     ref = g.ref["f64"]
     eng = _engine(g.job if form == "fp64" else g.job32, form)

@@ -73,7 +73,8 @@ def test_oracle_bit_identical_to_reference_f64(golden, oracle, name):
     for bit (same (f, F) float pairs in the same order)."""
     g = golden(name)
     pm, mm, nn = g.job.sky_points()
-    st, rec, per = refkit.search_points(oracle.orc_search_points, g.job.segment(), g.job.search_opts(), pm, mm, nn)
+    os_ = refkit.OracleSegment(g.job, oracle)   # the signal file injected, as main.c does
+    st, rec, per = refkit.search_points(oracle.orc_search_points, os_.seg, g.job.search_opts(), pm, mm, nn)
     assert st == 0
     ref = g.ref["f64"]
     assert len(rec) == len(ref)

@@ -51,7 +51,7 @@ UNIT = "templates/s"
 
 # ------------------------------------------------------------------ workload
 
-from tdfstat_b200.workloads import Workload, workload_case  # noqa: E402
+from tdfstat_b200.workloads import MultiWorkload, Workload, workload_case  # noqa: E402
 
 
 # ------------------------------------------------------------------ clocks
@@ -314,12 +314,116 @@ def run_tdf(args, rank, world, local_rank):
         shutil.rmtree(root, ignore_errors=True)
 
 
+def run_tdf_segments(args, rank, world, local_rank):
+    """cfg4: 64 segments of four sizes.  One engine per size, all on one
+    stream; a step streams every segment in (tdf_engine_upload: its inputs
+    from host memory) and searches its patch.  `value` includes the uploads
+    (the data of 64 segments is not resident at once); `e2e` also brings the
+    records back (tdf_search_points)."""
+    import torch
+    import torch.distributed as dist
+    from tdfstat_b200.engine import Engine
+
+    torch.cuda.set_device(local_rank)
+    root = tempfile.mkdtemp(prefix="tdfbench4_")
+    engines = {}
+    try:
+        mw = MultiWorkload(root, world=world)
+        shards = [(w,) + tuple(w.shard(rank, world)) for w in mw.segments]
+        stream = torch.cuda.Stream(device=local_rank)
+        tuned = {}
+        for w, pm, mm, nn in shards:
+            N = w.job.sett.N
+            if N not in engines:
+                e = Engine(w.job.segment(), w.job.search_opts(), form=args.form, device=local_rank,
+                           max_sky_batch=args.sky_batch)
+                e.set_stream(stream.cuda_stream)
+                tuned[N] = e.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
+                engines[N] = e
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+        def step(records=False):
+            n = 0
+            for w, pm, mm, nn in shards:
+                e = engines[w.job.sett.N]
+                e.upload(w.job.segment())
+                n += len(e.search(pm, mm, nn)) if records else e.search_device(pm, mm, nn)[0]
+            return n
+
+        def barrier():
+            if world > 1:
+                dist.barrier()
+
+        for _ in range(args.warmup):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            step()
+        torch.cuda.synchronize()
+        launches0 = sum(e.launch_count() for e in engines.values())
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        nsearched = 0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            nsearched += step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop()
+        ms = ev0.elapsed_time(ev1)
+        launches = sum(e.launch_count() for e in engines.values()) - launches0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nsearched_e2e = 0
+        for _ in range(args.steps):
+            nsearched_e2e += step(records=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e = e0.elapsed_time(e1)
+        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
+        n = torch.tensor([nsearched, nsearched_e2e], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        ms, ms_e2e = float(t[0]), float(t[1])
+        h2d = sum(sum(d.xdat.nbytes + d.detssb.nbytes for d in w.job.dets) + w.job.cosmodf.nbytes +
+                  w.job.sinmodf.nbytes for w, _, _, _ in shards)
+        if rank != 0:
+            return None
+        return {
+            "metric": METRIC, "value": round(float(n[0]) / (ms / 1e3), 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
+            "data": "synthetic (seeded Gaussian noise + injected CW signal per segment, synthetic ephemeris)",
+            "config": dict(mw.config, form=args.form, templates_per_chunk={str(k): v for k, v in tuned.items()},
+                           templates_searched_per_step=int(round(float(n[0]) / args.steps)),
+                           engines="one per segment size, segments streamed in by tdf_engine_upload each step",
+                           l2="flush: 256 MiB write between timed steps; per-step working set > L2"),
+            "e2e": {"value": round(float(n[1]) / (ms_e2e / 1e3), 1), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
+            "gpu_launches": int(launches),
+            "roofline": None, "cpu_baseline": None, "clocks": clk,
+        }
+    finally:
+        for e in engines.values():
+            e.close()
+        shutil.rmtree(root, ignore_errors=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
     root = tempfile.mkdtemp(prefix="tdfref_")
     try:
-        wl = Workload(args.workload, root)
+        # cfg4: the sample comes from its largest segment kind (nod 6, the 4th)
+        wl = Workload("cfg4:4" if args.workload == "cfg4" else args.workload, root)
         threads = os.cpu_count() or 1
         sroot = tempfile.mkdtemp(prefix="tdfrefs_")
         for _ in range(args.warmup):
@@ -353,7 +457,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tdf", choices=["tdf", "reference"])
     ap.add_argument("--form", default="split", choices=["split", "fp64"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--sky-batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
@@ -370,6 +474,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.workload == "cfg4":
+        out = run_tdf_segments(args, rank, world, local_rank)
     else:
         out = run_tdf(args, rank, world, local_rank)
     if world > 1 and args.impl == "tdf":

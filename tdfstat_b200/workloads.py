@@ -8,6 +8,13 @@
         grid cells) x 401 spindowns = 410,624 templates
   cfg3  as cfg2 with N = 258492 (6 days), nfft = 2^18, Ninterp = 2^19,
         a 128 x 64 patch (step 0.1 cells) x 401 spindowns = 3,284,992 templates
+  cfg4  64 segments, nod cycling through 2, 3, 4, 6 (N = 86164, 129246,
+        172328, 258492; nfft 2^17, 2^17, 2^18, 2^18), per-segment seeds, noise
+        and gaps, H1+L1; a 16 x 16 patch x 401 spindowns per segment =
+        6,569,984 templates (MultiWorkload)
+  cfg5  the scale configuration: H1+L1, N = 258492, sigma 1.0 / 1.3, 10% gaps,
+        801 spindowns; a 32 x 32 patch (2^10 points) = 820,224 templates
+        (larger skies scale the count, not the per-template work)
 All are seeded; the F range is the all-sky one, [nmin, nmax] (settings.c:83-84).
 """
 from __future__ import annotations
@@ -22,6 +29,17 @@ def workload_case(name: str):
     if name == "cfg1":
         return synth.Case(dt=2.0, nod=2, band=360, dets=("H1",), read_o3=True, seed=101, thr=14.5,
                           fdot_step=1e-10, sky_cells=16.0), (1, 1), 64, 0.25
+    if name == "cfg5":
+        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+        return synth.Case(dt=2.0, nod=6, band=360, dets=("H1", "L1"), sigma=(1.0, 1.3), gap_frac=0.10, seed=505,
+                          thr=14.5, fdot_step=1e-10, sky_cells=16.0, injections=(inj,)), (32, 32), 801, 0.1
+    if name.startswith("cfg4:"):
+        # one segment of cfg4: cfg4:<k>, k = 1..64
+        k = int(name.split(":")[1])
+        nod = (2, 3, 4, 6)[(k - 1) % 4]
+        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+        return synth.Case(seg=k, dt=2.0, nod=nod, band=360, dets=("H1", "L1"), seed=4000 + k, thr=14.5,
+                          fdot_step=1e-10, sky_cells=16.0, injections=(inj,)), (16, 16), 401, 0.1
     # the injections (and the patches centred on them) lie well inside the
     # sky grid's ellipse: every patch point is searched (job_core skips
     # points outside it, jobcore.c:248)
@@ -83,3 +101,21 @@ class Workload:
 
     def shard(self, rank: int, world: int):
         return shard_points(self.pm, self.mm, self.nn, rank, world)
+
+
+class MultiWorkload:
+    """cfg4: `nseg` segments (Workload "cfg4:<k>" each, under root/seg<k>),
+    grouped by their sizes so that one engine per size can take the
+    segments in turn."""
+
+    def __init__(self, root: str, nseg: int = 64, world: int = 1):
+        import os
+        self.segments = [Workload("cfg4:%d" % k, os.path.join(root, "seg%02d" % k), world)
+                         for k in range(1, nseg + 1)]
+        self.nspd = self.segments[0].nspd
+        self.templates = sum(w.templates for w in self.segments)
+        sizes = sorted({w.job.sett.N for w in self.segments})
+        self.config = {"workload": "cfg4", "detectors": "H1L1", "segments": nseg, "N": sizes,
+                       "nfft": sorted({w.job.sett.nfft for w in self.segments}),
+                       "sky_points_per_segment": len(self.segments[0].pm) // world, "spindowns": self.nspd,
+                       "templates_per_step": self.templates, "thr": self.segments[0].case.thr}

@@ -148,6 +148,35 @@ def cpu_reference_sample(wl: Workload, root: str, npts: int, threads: int):
     return len(recs), float(meta["walltime"])
 
 
+def cpu_fft_proxy(nfftf: int, threads: int, ntmpl: int, secs: float):
+    """The FFT share of a reference sample and the sample's rate with a
+    library-grade FFT in place of the project shim (FFTW is absent here):
+    2 single-precision transforms of nfftf per template (jobcore.c:477-478)
+    timed with the shim (fft_core.c, the reference's OpenMP threads) and with
+    scipy.fft (pocketfft, workers = threads).  The per-sky-point
+    interpolation transforms (FP64, 4 per detector per point) are left in."""
+    import time as _t
+    import numpy as _np
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import refkit
+    try:
+        import scipy.fft as sfft
+    except ImportError:
+        return None
+    t_shim = float(refkit.load_oracle().orc_fft_time_f(nfftf, 20))
+    x = (_np.random.default_rng(0).standard_normal(nfftf) + 1j * _np.random.default_rng(1).standard_normal(nfftf))
+    x = x.astype(_np.complex64)
+    sfft.fft(x, workers=threads)
+    t0 = _t.perf_counter()
+    for _ in range(20):
+        sfft.fft(x, workers=threads)
+    t_sp = (_t.perf_counter() - t0) / 20
+    fft_s = 2 * ntmpl * t_shim
+    return {"fft_share": round(fft_s / secs, 3), "shim_ms_per_fft": round(1e3 * t_shim, 3),
+            "scipy_ms_per_fft": round(1e3 * t_sp, 3),
+            "value_with_scipy_fft": round(ntmpl / max(secs - 2 * ntmpl * (t_shim - t_sp), 1e-9), 2)}
+
+
 # ------------------------------------------------------------------ arms
 
 def run_tdf(args, rank, world, local_rank):
@@ -289,6 +318,7 @@ def run_tdf(args, rank, world, local_rank):
                     nrec_c, secs = r
                     cpu = {"value": round(nrec_c / secs, 2), "unit": UNIT, "cores": os.cpu_count(),
                            "kind": "reference",
+                           "fft": cpu_fft_proxy(job.sett.nfftf, os.cpu_count() or 1, nrec_c, secs),
                            "sample": "%d templates (3 sky points x %d spindowns) of the same workload, reference "
                                      "search sources PREC=FLOAT built with the project FFTW-API shim "
                                      "(textbook radix-2 FFT; FFTW absent), %.1f s" % (nrec_c, wl.nspd, secs)}
@@ -436,6 +466,7 @@ def run_reference(args, rank, world):
             tot_n += n
             tot_s += s
         v = tot_n / tot_s
+        fftp = cpu_fft_proxy(wl.job.sett.nfftf, threads, tot_n, tot_s)
         sample = ("%d templates per step (1 sky point x %d spindowns) of the %s workload; reference search "
                   "sources (PREC=FLOAT, SIMD=NONE) compiled unmodified against the project FFTW-API shim "
                   "(textbook radix-2 FFT, FFTW absent)" % (tot_n // args.steps, wl.nspd, wl.name))
@@ -444,7 +475,7 @@ def run_reference(args, rank, world):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic", "config": dict(wl.config),
                 "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "cores": threads, "kind": "reference",
-                                 "sample": sample},
+                                 "sample": sample, "fft": fftp},
                 "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     finally:
         shutil.rmtree(root, ignore_errors=True)

@@ -152,18 +152,24 @@ def cpu_fft_proxy(nfftf: int, threads: int, ntmpl: int, secs: float):
     """The FFT share of a reference sample and the sample's rate with a
     library-grade FFT in place of the project shim (FFTW is absent here):
     2 single-precision transforms of nfftf per template (jobcore.c:477-478)
-    timed with the shim (fft_core.c, the reference's OpenMP threads) and with
-    scipy.fft (pocketfft, workers = threads).  The per-sky-point
+    timed with the shim as the reference binary has it (oracle/_ref/
+    fft-time-f32: same flags, `threads` OpenMP threads, own process) and
+    with scipy.fft (pocketfft, workers = threads).  The per-sky-point
     interpolation transforms (FP64, 4 per detector per point) are left in."""
     import time as _t
     import numpy as _np
-    sys.path.insert(0, os.path.join(REPO, "tests"))
-    import refkit
     try:
         import scipy.fft as sfft
     except ImportError:
         return None
-    t_shim = float(refkit.load_oracle().orc_fft_time_f(nfftf, 20))
+    exe = os.path.join(REPO, "oracle", "_ref", "fft-time-f32")
+    if not os.path.exists(exe):
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([exe, str(nfftf), "50"], capture_output=True, text=True, env=env, timeout=120)
+    if r.returncode != 0:
+        return None
+    t_shim = float(r.stdout.split()[0])
     x = (_np.random.default_rng(0).standard_normal(nfftf) + 1j * _np.random.default_rng(1).standard_normal(nfftf))
     x = x.astype(_np.complex64)
     sfft.fft(x, workers=threads)

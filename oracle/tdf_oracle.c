@@ -12,7 +12,6 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
-#include <time.h>
 
 #include "fft_core.h"
 #include "tdf_oracle.h"
@@ -477,20 +476,4 @@ int orc_fstat_spectrum(const tdf_segment *seg, const tdf_search_opts *opts,
      fftc_plan_destroy(plan);
      free(xam); free(xbm); free(tmp1); free(shft); free(fxa); free(fxb); free(F);
      return TDF_OK;
-}
-
-double orc_fft_time_f(int n, int reps)
-{
-     fftc_plan *p = fftc_plan_create(n, -1);
-     if (!p || reps < 1) return -1.;
-     float complex *x = (float complex *)malloc((size_t)n * sizeof(float complex));
-     for (int i = 0; i < n; i++) x[i] = CMPLXF((float)((i * 7) % 13) - 6.f, (float)((i * 5) % 11) - 5.f);
-     fftc_execute_f(p, x, x);   /* warm */
-     struct timespec t0, t1;
-     clock_gettime(CLOCK_MONOTONIC, &t0);
-     for (int r = 0; r < reps; r++) fftc_execute_f(p, x, x);
-     clock_gettime(CLOCK_MONOTONIC, &t1);
-     free(x);
-     fftc_plan_destroy(p);
-     return ((double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec)) / reps;
 }

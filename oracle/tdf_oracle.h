@@ -54,12 +54,6 @@ void orc_splintpad(const double complex *ya, const double *shftf, int N,
    else 0; *h0 receives the amplitude used. */
 int orc_add_signal(const tdf_segment *seg, const tdf_signal *sig, double *h0);
 
-/* Seconds per in-place single-precision transform of length n by the FFT
-   the reference binaries are linked with here (fft_core.c behind the FFTW
-   shim), averaged over reps, with the process's OpenMP threads; bench.py's
-   CPU-baseline leg uses it to report the FFT share of the reference's time. */
-double orc_fft_time_f(int n, int reps);
-
 /* textbook FFT (fft_core.c), exposed for the FFT tests */
 int orc_fft(int n, int sign, const double complex *in, double complex *out);
 

@@ -151,8 +151,6 @@ def load_oracle():
     lib.orc_fft.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     lib.orc_splintpad.restype = None
     lib.orc_splintpad.argtypes = [C.c_void_p, _abi.F64P, C.c_int, C.c_int, C.c_void_p]
-    lib.orc_fft_time_f.restype = C.c_double
-    lib.orc_fft_time_f.argtypes = [C.c_int, C.c_int]
     lib.orc_add_signal.restype = C.c_int
     lib.orc_add_signal.argtypes = [C.c_void_p, C.POINTER(_abi.TdfSignal), C.POINTER(C.c_double)]
     return lib

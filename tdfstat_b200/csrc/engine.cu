@@ -103,7 +103,7 @@ static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T
      }
      auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi>;
      TRY(set_smem(kern, smem));
-     kern<<<grid, L, smem, st>>>(pro, epi, tw);
+     kern<<<grid, pass_threads<L>(), smem, st>>>(pro, epi, tw);
      CUCHK(cudaGetLastError());
      return TDF_OK;
 }
@@ -120,7 +120,7 @@ static int launch_row_L(dim3 grid, const Src &src_in, const Epi &epi, const cx<T
      }
      auto kern = k_rowpass<T, L, SIGN, NA, Src, Epi>;
      TRY(set_smem(kern, smem));
-     kern<<<grid, L, smem, st>>>(src, epi, tw);
+     kern<<<grid, pass_threads<L>(), smem, st>>>(src, epi, tw);
      CUCHK(cudaGetLastError());
      return TDF_OK;
 }

@@ -17,6 +17,10 @@
 
 namespace tdf {
 
+// threads of a pass CTA: L/8 per line, LINES lines
+template <int L>
+constexpr int pass_threads() { return L / 8 * LINES; }
+
 template <typename T, int L, int NA>
 constexpr size_t pass_smem_bytes() {
      return sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
@@ -60,7 +64,7 @@ template <class P>
 struct has_tables<P, std::void_t<decltype(P::kTables)>> : std::integral_constant<bool, P::kTables> {};
 
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
-__global__ void __launch_bounds__(L, (pass_min_blocks<T, L>()))
+__global__ void __launch_bounds__(pass_threads<L>(), (pass_min_blocks<T, L>()))
 k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
      extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -90,7 +94,7 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
 }
 
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
-__global__ void __launch_bounds__(L, (row_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
+__global__ void __launch_bounds__(pass_threads<L>(), (row_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
      using G = LineGeom<T, L>;
      extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);

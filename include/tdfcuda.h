@@ -194,6 +194,59 @@ int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0, int3
    included) to the host. */
 int tdf_engine_get_xdat(tdf_engine *e, int32_t det, float *xdat, int64_t n);
 
+/* ---- coincidences between segments (coincidences/coincidences.c) ---- */
+
+/* The options of the reference's [coincidences] INI section (io.c:86-154). */
+typedef struct tdf_coinc_opts {
+     int32_t refr;        /* reference segment: trigger frequencies are moved to it */
+     double cthr;         /* F-statistic threshold */
+     int32_t scalef;      /* cell size in frequency, in bins of pi/nfftf */
+     int32_t scales, scalem, scalen;   /* cell sizes in grid steps */
+     int32_t mincoin;     /* segments a coincidence needs (>= 1) */
+     int32_t shift;       /* -1: the 16 cell shifts 0..15; else that one (bits m,n,s,f = 8,4,2,1) */
+} tdf_coinc_opts;
+
+/* One segment's search: what the reference reads from its trigger file.
+   Every segment must hold the same templates in the same order (the same
+   grid and search range); the template headers are taken from segment 0. */
+typedef struct tdf_coinc_segment {
+     int32_t seg;               /* segment number (opts.seg of that search) */
+     int32_t N, nfftf;          /* sett.N, sett.nfftf (nfftf equal in all segments) */
+     double dt, narrowdown;     /* sett.dt; opts.narrowdown [rad] */
+     int32_t nlines;            /* veto intervals, [nlines][2] in units of f (0..pi) */
+     const double *lines;
+     int64_t nrec;              /* its records, as tdf_search_points() returns them */
+     const tdf_record *recs;
+     const float *pairs;
+} tdf_coinc_segment;
+
+typedef struct tdf_coincidence {
+     int32_t shift;             /* 0..15, bits m,n,s,f = 8,4,2,1 (the reference's "mnsf" string) */
+     int32_t w;                 /* segments in the coincidence */
+     float avg_snr, avg_f, avg_fdot, avg_ra, avg_dec;
+     int64_t member;            /* its w members start here in cseg[], trig[], ntrig[] */
+} tdf_coincidence;
+
+/* The coincidence search of coincidences.c:44-436 over nseg segments: per
+   segment the triggers with F >= cthr inside the narrow-down window and
+   outside the veto lines, moved to segment refr by their spindown
+   (select_goodcands, :439-503); per shift the (m, n, s) cells of the
+   templates, the loudest trigger per (cell, segment, frequency cell), and a
+   coincidence wherever >= mincoin segments share a frequency cell.  Output,
+   shift by shift in increasing order, each shift's coincidences in the
+   reference's order (more segments first, then higher mean SNR): coi[] and
+   their members (segment index cseg, template index trig, triggers in the
+   cell ntrig); seginfo[nshift][nseg][3] = {segment number, selected
+   triggers, unique triggers of the shift}.  If max_coi or max_members is too
+   small nothing is written, *ncoi and *nmembers receive the sizes needed and
+   the call returns TDF_ERR_CAPACITY.  Runs on the host; no device is needed.
+   Extension of this library: the reference is a separate program reading
+   HDF5 trigger files. */
+int tdf_coincidences(const tdf_coinc_opts *opts, int32_t nseg, const tdf_coinc_segment *segs,
+                     tdf_coincidence *coi, int64_t max_coi, int64_t *ncoi,
+                     int16_t *cseg, int32_t *trig, int16_t *ntrig, int64_t max_members, int64_t *nmembers,
+                     int32_t *seginfo);
+
 /* F-statistic of one template of the split form from spindown operands that
    are already on the device, without allocating any memory.  No counterpart
    in the reference: it is for callers that must not allocate device memory

@@ -104,6 +104,47 @@ class TdfSignal(C.Structure):
     ]
 
 
+class TdfCoincOpts(C.Structure):
+    _fields_ = [
+        ("refr", C.c_int32),
+        ("cthr", C.c_double),
+        ("scalef", C.c_int32),
+        ("scales", C.c_int32),
+        ("scalem", C.c_int32),
+        ("scalen", C.c_int32),
+        ("mincoin", C.c_int32),
+        ("shift", C.c_int32),
+    ]
+
+
+class TdfCoincSegment(C.Structure):
+    _fields_ = [
+        ("seg", C.c_int32),
+        ("N", C.c_int32),
+        ("nfftf", C.c_int32),
+        ("dt", C.c_double),
+        ("narrowdown", C.c_double),
+        ("nlines", C.c_int32),
+        ("lines", C.POINTER(C.c_double)),
+        ("nrec", C.c_int64),
+        ("recs", C.POINTER(TdfRecord)),
+        ("pairs", C.POINTER(C.c_float)),
+    ]
+
+
+class TdfCoincidence(C.Structure):
+    _fields_ = [
+        ("shift", C.c_int32),
+        ("w", C.c_int32),
+        ("avg_snr", C.c_float),
+        ("avg_f", C.c_float),
+        ("avg_fdot", C.c_float),
+        ("avg_ra", C.c_float),
+        ("avg_dec", C.c_float),
+        ("member", C.c_int64),
+    ]
+
+
 class TdfKernelTimes(C.Structure):
     _fields_ = [
         ("colpass_ms", C.c_double),
@@ -144,6 +185,9 @@ ABI_FUNCTIONS = [
      [P, C.c_int32, C.c_float, C.c_float, C.c_float, F64P, C.c_int64]),
     ("tdf_engine_add_signal", C.c_int, [P, C.POINTER(TdfSignal), F64P, I32P]),
     ("tdf_engine_get_xdat", C.c_int, [P, C.c_int32, F32P, C.c_int64]),
+    ("tdf_coincidences", C.c_int,
+     [C.POINTER(TdfCoincOpts), C.c_int32, C.POINTER(TdfCoincSegment), C.POINTER(TdfCoincidence), C.c_int64, I64P,
+      C.POINTER(C.c_int16), I32P, C.POINTER(C.c_int16), C.c_int64, I64P, I32P]),
     ("tdf_fstat_operands_static", C.c_int,
      [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_float, C.c_float,
       C.c_int32, C.c_int32, P, P]),

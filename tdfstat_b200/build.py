@@ -15,7 +15,7 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libtdfcuda.so")
-SOURCES = ["engine.cu", "refabi.cu"]
+SOURCES = ["engine.cu", "refabi.cu", "coinc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

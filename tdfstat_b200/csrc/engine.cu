@@ -40,6 +40,17 @@ static int set_error(int code, const char *fmt, ...) {
      return code;
 }
 
+// the same for the library's other sources
+int tdf_internal_set_error(int code, const char *fmt, ...) {
+     char buf[1024];
+     va_list ap;
+     va_start(ap, fmt);
+     vsnprintf(buf, sizeof(buf), fmt, ap);
+     va_end(ap);
+     g_last_error = buf;
+     return code;
+}
+
 #define CUCHK(x)                                                                          \
      do {                                                                                 \
           cudaError_t e_ = (x);                                                           \

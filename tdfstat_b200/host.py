@@ -562,6 +562,7 @@ class Job:
         if narrowdown < 0.:
             narrowdown = (1. - overlap) / 2.
         narrowdown *= math.pi
+        self.narrowdown = narrowdown          # opts->narrowdown [rad] (init.c:134-139)
         self.usedet = ini.get("search:usedet", "")
         self.mods = ini.get("search:mods", "")
         self.fstat_norm = ini.get("search:fstat_norm", "")

@@ -83,6 +83,7 @@ class Case:
     vlines_hz: Sequence[Sequence[float]] = ()   # veto intervals [Hz]
     injections: Sequence[Injection] = ()
     addsig: Optional[Injection] = None          # written as the reference's signal file, not applied
+    noise_seed: Optional[int] = None            # set: noise from its own generator (segments sharing a grid)
     label: str = ""
 
     def settings(self) -> host.Settings:
@@ -224,12 +225,13 @@ def write_case(root: str, case: Case) -> str:
     orbit_phase = rng.uniform(0, 2 * math.pi)
     gmst0 = rng.uniform(0, 2 * math.pi)
     dets, xs = [], []
+    nrng = rng if case.noise_seed is None else np.random.default_rng(case.noise_seed)
     for k, name in enumerate(case.dets):
         elam = host.detector_geometry(name)[1]
         phir = math.fmod(gmst0 + elam + 2 * math.pi, 2 * math.pi)
         e = detssb(N, case.dt, name, phir, orbit_phase)
         sigma = case.sigma[k] if k < len(case.sigma) else case.sigma[-1]
-        x = noise(N, sigma, case.gap_frac, case.ngaps, rng)
+        x = noise(N, sigma, case.gap_frac, case.ngaps, nrng)
         d = host.Detector(name=name, xdat=x.astype(np.float32), detssb=e, phir=phir, epsm=host.C_EPSMA).finish()
         dets.append(d)
         xs.append(x)

@@ -47,6 +47,46 @@ CASES = {
 }
 
 
+# Coincidences between segments (coincidences/coincidences.c): segments 1-4
+# of one search (same grid and range, one INI per segment, noise per
+# segment) with a signal (network SNR 14 per segment) whose frequency moves
+# with its spindown; the reference's coincidence program runs on the
+# reference's trigger files with each option set
+COINC_CASES = {
+    "c1_4seg": {
+        "base": synth.Case(
+            dt=8.0, nod=1, band=1440, dets=("H1", "L1"), sigma=(1.0, 1.1), seed=55, thr=6.5,
+            fdot_step=2e-10, sky_cells=12.0, gtype="allsky_range",
+            gcenter=(100.031, -4e-10, 2.1, -0.4), gsizes=(3600, 5.0, 1.0, 1.0), gsteps=(1, 1.0, 1.0, 1.0),
+            injections=(synth.Injection(f=100.031, fdot=-4e-10, ra=2.1, dec=-0.4, iota=0.6, psi=0.2, phase=0.9,
+                                        snr=14.0),)),
+        "segs": (1, 2, 3, 4),
+        "noise_seed": 5500,          # segment k: noise_seed + k
+        "hemi": 2,                   # the hemisphere whose trigger files are compared
+        "opts": {
+            "a": dict(refr=2, cthr=7.0, scalef=4, scales=1, scalem=1, scalen=1, mincoin=2),
+            "b": dict(refr=1, cthr=7.0, scalef=8, scales=2, scalem=2, scalen=2, mincoin=3),
+        },
+    },
+}
+
+
+def write_coinc_case(root: str, name: str):
+    """Writes the segments of a coincidence case under `root` (one INI per
+    segment, search_<seg>.ini); returns [(seg, ini path)]."""
+    import dataclasses
+    import shutil
+    cc = COINC_CASES[name]
+    out = []
+    for seg in cc["segs"]:
+        c = dataclasses.replace(cc["base"], seg=seg, noise_seed=cc["noise_seed"] + seg)
+        ini = synth.write_case(root, c)
+        segini = os.path.join(root, "search_%03d.ini" % seg)
+        shutil.copy(ini, segini)
+        out.append((seg, segini))
+    return out
+
+
 def input_checksum(root: str) -> str:
     """sha256 over the input files of a written case (sorted paths)."""
     h = hashlib.sha256()

@@ -61,5 +61,53 @@ def main(names=None):
             shutil.rmtree(root, ignore_errors=True)
 
 
+def main_coinc(names=None):
+    """Coincidence fixtures: the reference's search (FP64 build) on every
+    segment, then its coincidence program (oracle/_ref/coinc-ref) on the
+    segments' trigger files of one hemisphere, once per option set."""
+    import subprocess
+    from golden.cases import COINC_CASES, write_coinc_case
+    refkit.build_oracle(ref=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"), "coinc"],
+                   check=True)
+    for name, cc in COINC_CASES.items():
+        if names and name not in names:
+            continue
+        root = tempfile.mkdtemp(prefix="tdfgoldc_")
+        try:
+            segs = write_coinc_case(root, name)
+            out = {"checksum": np.array(input_checksum(root))}
+            files = []
+            for seg, ini in segs:
+                refkit.run_reference(ini, "f64", threads=1)
+                files.append("out/triggers_%03d_%04d_%d.h5" % (seg, cc["base"].band, cc["hemi"]))
+            for key, o in cc["opts"].items():
+                odir = os.path.join(root, "coin_" + key)
+                os.makedirs(odir, exist_ok=True)
+                ini = os.path.join(root, "coinc_%s.ini" % key)
+                with open(ini, "w") as f:
+                    f.write("[coincidences]\n")
+                    for k, v in o.items():
+                        f.write("%s = %r\n" % (k, v))
+                    f.write("hemi = %d\nout_dir = %s\ntrig_file_list = %s\n" % (cc["hemi"], odir, " ".join(files)))
+                subprocess.run([refkit.REF_BIN["coinc"], ini], cwd=root, check=True, capture_output=True)
+                cf = [fn for fn in os.listdir(odir) if fn.startswith("coin_")]
+                coin = refkit.read_coin_file(os.path.join(odir, cf[0]))
+                for ish, blk in coin.items():
+                    p = "%s_%02d_" % (key, ish)
+                    cois = blk["coi"]
+                    out[p + "seginfo"] = blk["seginfo"]
+                    out[p + "w"] = np.array([c[0] for c in cois], dtype=np.int16)
+                    out[p + "vals"] = np.array([c[1:6] for c in cois], dtype=np.float32).reshape(-1, 5)
+                    out[p + "cseg"] = np.concatenate([c[6] for c in cois]) if cois else np.zeros(0, np.int16)
+                    out[p + "trig"] = np.concatenate([c[7] for c in cois]) if cois else np.zeros(0, np.int32)
+                    out[p + "ntrig"] = np.concatenate([c[8] for c in cois]) if cois else np.zeros(0, np.int16)
+                print("%-10s %s: %s coincidences over 16 shifts" % (name, key, sum(len(b["coi"]) for b in coin.values())))
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        finally:
+            shutil.rmtree(root, ignore_errors=True)
+
+
 if __name__ == "__main__":
     main(sys.argv[1:])
+    main_coinc(sys.argv[1:])

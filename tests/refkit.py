@@ -23,6 +23,7 @@ REF_BIN = {
     "f64": os.path.join(ORACLE_DIR, "_ref", "gwsearch-ref-f64"),
     "f32": os.path.join(ORACLE_DIR, "_ref", "gwsearch-ref-f32"),
     "dropin": os.path.join(ORACLE_DIR, "_ref", "gwsearch-dropin"),
+    "coinc": os.path.join(ORACLE_DIR, "_ref", "coinc-ref"),
 }
 ORACLE_LIB = os.path.join(ORACLE_DIR, "libtdforacle.so")
 
@@ -67,11 +68,23 @@ def read_trigger_file(path: str) -> Tuple[Records, Dict]:
     """Reads the flat trigger file written by oracle/ref_io.c."""
     with open(path, "rb") as f:
         data = f.read()
-    assert data[:8] == b"TDFTRIG2", path
+    assert data[:8] in (b"TDFTRIG2", b"TDFTRIG3"), path
     ver, nifo = struct.unpack_from("<ii", data, 8)
     off = 16
     hdrs, pairs = [], []
     meta = {"format_version": ver, "nifo": nifo}
+    if ver >= 3:
+        band, seg, hemi = struct.unpack_from("<3i", data, off)
+        overlap, narrowdown = struct.unpack_from("<2d", data, off + 12)
+        gl = struct.unpack_from("<I", data, off + 28)[0]
+        grid_file = data[off + 32: off + 32 + gl].decode()
+        off += 32 + gl
+        fpo, dt, B = struct.unpack_from("<3d", data, off)
+        nod, N, nfftf, numlines_band, nvl = struct.unpack_from("<5i", data, off + 24)
+        off += 44
+        meta.update(band=band, seg=seg, hemi=hemi, overlap=overlap, narrowdown=narrowdown, grid_file=grid_file,
+                    fpo=fpo, dt=dt, B=B, nod=nod, N=N, nfftf=nfftf, numlines_band=numlines_band,
+                    nvlines_all_inband=nvl)
     while off < len(data):
         h = struct.unpack_from("<6f", data, off)
         ln = struct.unpack_from("<I", data, off + 24)[0]
@@ -85,6 +98,39 @@ def read_trigger_file(path: str) -> Tuple[Records, Dict]:
         hdrs.append(h)
         pairs.append(p)
     return Records(np.array(hdrs, dtype=np.float32).reshape(-1, 6), pairs), meta
+
+
+def read_coin_file(path: str) -> Dict[int, Dict]:
+    """Reads the flat coincidence file of oracle/coinc_io.c: per shift (as
+    the integer of its 'mnsf' bit string) its seginfo [nseg][3] and its
+    coincidences (w, avg_snr, avg_f, avg_fdot, avg_ra, avg_dec, cseg, trig,
+    ntrig) in file order."""
+    with open(path, "rb") as f:
+        data = f.read()
+    assert data[:8] == b"TDFCOIN1", path
+    nseg = struct.unpack_from("<i", data, 8)[0]
+    off = 12
+    out = {}
+    while off < len(data):
+        shift = int(data[off:off + 4].decode(), 2)
+        icoi = struct.unpack_from("<i", data, off + 5)[0]
+        off += 9
+        seginfo = np.frombuffer(data, dtype="<i4", count=3 * nseg, offset=off).reshape(nseg, 3).copy()
+        off += 12 * nseg
+        cois = []
+        for _ in range(icoi):
+            w = struct.unpack_from("<h", data, off)[0]
+            vals = struct.unpack_from("<5f", data, off + 2)
+            off += 22
+            cseg = np.frombuffer(data, dtype="<i2", count=w, offset=off).copy()
+            off += 2 * w
+            trig = np.frombuffer(data, dtype="<i4", count=w, offset=off).copy()
+            off += 4 * w
+            ntrig = np.frombuffer(data, dtype="<i2", count=w, offset=off).copy()
+            off += 2 * w
+            cois.append((w,) + tuple(np.float32(v) for v in vals) + (cseg, trig, ntrig))
+        out[shift] = {"seginfo": seginfo, "coi": cois}
+    return out
 
 
 def _big_stack():

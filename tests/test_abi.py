@@ -60,10 +60,12 @@ def _c_sizeof(header, types):
 
 
 def test_struct_layouts_match_c():
-    types = ["tdf_detector", "tdf_segment", "tdf_search_opts", "tdf_record", "tdf_kernel_times"]
+    types = ["tdf_detector", "tdf_segment", "tdf_search_opts", "tdf_record", "tdf_kernel_times", "tdf_signal",
+             "tdf_coinc_opts", "tdf_coinc_segment", "tdf_coincidence"]
     sizes = _c_sizeof("tdfcuda.h", types)
     py = [C.sizeof(t) for t in (_abi.TdfDetector, _abi.TdfSegment, _abi.TdfSearchOpts, _abi.TdfRecord,
-                                _abi.TdfKernelTimes)]
+                                _abi.TdfKernelTimes, _abi.TdfSignal, _abi.TdfCoincOpts, _abi.TdfCoincSegment,
+                                _abi.TdfCoincidence)]
     assert sizes == py
 
 

@@ -208,8 +208,10 @@ struct RowsY {
 
 // RowsY<T, 2> with the CTA's LINES rows brought in by bulk copies: row r
 // (N2 elements of 2 cx<T>, both arrays) goes to shared offset
-// r * (EB*N2 + 64), so that the 8 rows a warp reads from at once do not all
-// start on the same bank; the slots alias the line buffers, which the first
+// r * (EB*N2 + 16).  A 16-byte load is served 8 lanes at a time, here the 8
+// rows at one element; the 16-byte pad puts those on 8 different 16-byte
+// bank groups (EB*N2 is a multiple of 128).  The slots alias the line
+// buffers, which the first
 // pass only writes after k_rowpass's barrier that follows the reads.  Thread
 // 0 issues the copies; everyone waits on one mbarrier (bounded: on time-out
 // ERR_STAGE_TIMEOUT is or-ed into *err).
@@ -221,7 +223,7 @@ struct RowsYBulk {
      unsigned *err;
      unsigned bar_off = 0;   // byte offset of the barrier in dynamic shared memory (set by the launcher)
      static constexpr bool kBulk = true;
-     static constexpr unsigned kPad = 64;
+     static constexpr unsigned kPad = 16;
      static constexpr unsigned EB = 2 * sizeof(cx<T>);   // bytes of an element, both arrays
 
      template <int L>

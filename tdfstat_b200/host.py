@@ -23,6 +23,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import _abi
+from . import vlines as vlines_mod
 
 # common.h:14-31
 RAD_TO_DEG = 180.0 / math.pi
@@ -497,22 +498,7 @@ def sky_points(rng: SearchRange):
 
 
 # ---------------------------------------------------------------- veto lines
-
-def narrow_down_lines(narrowdown: float):
-    """common.c:433-445"""
-    return [[0.0, math.pi / 2 - narrowdown], [math.pi / 2 + narrowdown, math.pi]]
-
-
-def read_band_vlines(path: str) -> List[List[float]]:
-    """common.c:477-553: veto intervals [rad] of a vlines_BBBB.dat file."""
-    out = []
-    with open(path) as f:
-        for line in f:
-            if line.startswith("#") or not line.strip():
-                continue
-            a = line.split()
-            out.append([float(a[0]), float(a[1])])
-    return out
+# narrow_down_band, read_band_vlines, extract_band_vlines: tdfstat_b200/vlines.py
 
 
 # ---------------------------------------------------------------- the job
@@ -543,11 +529,18 @@ class Job:
     but not applied: the engine applies it on the device
     (Engine.add_signal), as main.c:101-104 does on the host."""
 
-    def __init__(self, ini_path: str, float_build: bool = True):
+    def __init__(self, ini_path: str, float_build: bool = True, vlines: str = "auto"):
+        """`vlines`: "auto" reads <outdir>/vlines_<band><label>.dat when it
+        exists and otherwise extracts the band's veto lines from
+        <indir>/lines/ and writes that file (main.c:84-94); "extract" always
+        extracts and writes it (vlinegen.c:66-78)."""
+        if vlines not in ("auto", "extract"):
+            raise ValueError("vlines must be 'auto' or 'extract'")
         self.ini_path = ini_path
         ini = read_ini(ini_path)
         self.ini = ini
         indir = ini["search:indir"]
+        indir_ini = indir
         base = os.path.dirname(os.path.abspath(ini_path))
         if not os.path.isabs(indir):
             indir = os.path.join(base, indir)
@@ -601,17 +594,19 @@ class Job:
         self.sett.nifo = len(self.dets)
         self.sett.sepsm = self.dets[-1].sepsm
         self.sett.cepsm = self.dets[-1].cepsm
-        lines: List[List[float]] = []
-        if narrowdown < 0.5 * math.pi:
-            lines = narrow_down_lines(narrowdown)
-        numlines = len(lines)
-        vl = os.path.join(outdir, "vlines_%04d%s.dat" % (self.band, self.label))
-        if os.path.exists(vl):
-            lines = lines + read_band_vlines(vl)
-            if self.veto_flag:
-                numlines = len(lines)
-        self.lines = lines
-        self.numlines = numlines
+        # main.c:78-94
+        narrow = vlines_mod.narrow_down_lines(narrowdown) if narrowdown < 0.5 * math.pi else []
+        os.makedirs(outdir, exist_ok=True)                 # main.c:53-64
+        self.vlines_file = os.path.join(outdir, "vlines_%04d%s.dat" % (self.band, self.label))
+        if vlines == "auto" and os.access(self.vlines_file, os.R_OK):
+            bv = vlines_mod.read_band_vlines(self.vlines_file, narrow, self.veto_flag)
+        else:
+            bv = vlines_mod.extract_band_vlines(
+                self.sett.fpo, self.sett.B, N, self.sett.dt, [d.detssb for d in self.dets],
+                [d.name for d in self.dets], indir_ini, narrow, self.veto_flag, self.vlines_file, base=base)
+        self.vlines = bv
+        self.lines = bv.lines
+        self.numlines = bv.numlines_band
         self.cosmodf, self.sinmodf = aux_arrays(N, self.sett.omr)
         self.range = set_search_range(self.sett, ini, float_build=float_build)
         self.sett.bufsize = self.sett.nfftf // 16 if self.gtype == "allsky" else self.sett.nfftf
@@ -673,3 +668,11 @@ class Job:
 
     def sky_points(self):
         return sky_points(self.range)
+
+
+def vlinegen(ini_path: str) -> str:
+    """vlinegen.c: extracts the veto lines of the INI's band from the line
+    lists under <indir>/lines/ and (over)writes <outdir>/vlines_<band><label>.dat,
+    the file a later search reads; returns its path."""
+    return Job(ini_path, vlines="extract").vlines_file
+

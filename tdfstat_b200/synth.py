@@ -81,6 +81,7 @@ class Case:
     narrowdown: float = -1.0
     veto_flag: int = 0
     vlines_hz: Sequence[Sequence[float]] = ()   # veto intervals [Hz]
+    line_files: Sequence[Sequence[str]] = ()    # (name, text) of line lists under <indir>/lines/
     injections: Sequence[Injection] = ()
     addsig: Optional[Injection] = None          # written as the reference's signal file, not applied
     noise_seed: Optional[int] = None            # set: noise from its own generator (segments sharing a grid)
@@ -251,6 +252,12 @@ def write_case(root: str, case: Case) -> str:
         with open(os.path.join(ddir, "starting_date"), "w") as f:
             f.write("1.2000000000e+09\n")
     label = ("_" + case.label) if case.label else ""
+    if case.line_files:
+        ldir = os.path.join(indir, "lines")
+        os.makedirs(ldir, exist_ok=True)
+        for name, text in case.line_files:
+            with open(os.path.join(ldir, name), "w") as f:
+                f.write(text)
     if case.vlines_hz:
         with open(os.path.join(outdir, "vlines_%04d%s.dat" % (case.band, label)), "w") as f:
             f.write("# fl[rad]  fr[rad]   fl[Hz]  fr[Hz]   line info\n")

@@ -108,6 +108,29 @@ def main_coinc(names=None):
             shutil.rmtree(root, ignore_errors=True)
 
 
+def main_vlines(names=None):
+    """Veto-line fixtures: the veto file the reference's vlinegen program
+    writes for each case of VLINE_CASES, as text (<name>.vlines)."""
+    import subprocess
+    from golden.cases import VLINE_CASES
+    subprocess.run(["make", "-s", "-C", os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"), "vlinegen"],
+                   check=True)
+    for name, case in VLINE_CASES.items():
+        if names and name not in names:
+            continue
+        root = tempfile.mkdtemp(prefix="tdfgoldv_")
+        try:
+            ini = synth.write_case(root, case)
+            text = refkit.run_vlinegen(ini)
+            with open(os.path.join(HERE, name + ".vlines"), "w", encoding="latin-1") as f:
+                f.write("# input checksum %s\n" % input_checksum(root))
+                f.write(text)
+            print("%-12s %d veto lines" % (name, sum(1 for ln in text.splitlines() if not ln.startswith("#"))))
+        finally:
+            shutil.rmtree(root, ignore_errors=True)
+
+
 if __name__ == "__main__":
     main(sys.argv[1:])
     main_coinc(sys.argv[1:])
+    main_vlines(sys.argv[1:])

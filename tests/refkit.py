@@ -10,6 +10,7 @@ import ctypes as C
 import glob
 import os
 import struct
+import re
 import subprocess
 from typing import Dict, List, Optional, Tuple
 
@@ -24,6 +25,7 @@ REF_BIN = {
     "f32": os.path.join(ORACLE_DIR, "_ref", "gwsearch-ref-f32"),
     "dropin": os.path.join(ORACLE_DIR, "_ref", "gwsearch-dropin"),
     "coinc": os.path.join(ORACLE_DIR, "_ref", "coinc-ref"),
+    "vlinegen": os.path.join(ORACLE_DIR, "_ref", "vlinegen-ref"),
 }
 ORACLE_LIB = os.path.join(ORACLE_DIR, "libtdforacle.so")
 
@@ -173,6 +175,19 @@ def run_reference(ini: str, which: str = "f64", threads: int = 1, timeout: float
     hdr = np.concatenate(hdrs) if hdrs else np.zeros((0, 6), np.float32)
     pm = np.concatenate(pms) if pms else np.zeros(0, np.int32)
     return Records(hdr, pairs, pm), meta, out.stdout
+
+
+def run_vlinegen(ini: str, timeout: float = 600) -> str:
+    """Runs the reference's veto-line generator (vlinegen.c) on `ini`
+    (cwd = the INI's directory); returns the text of the veto file it wrote."""
+    wd = os.path.dirname(os.path.abspath(ini))
+    out = subprocess.run([REF_BIN["vlinegen"], os.path.basename(ini)], cwd=wd, capture_output=True,
+                         text=True, timeout=timeout, preexec_fn=_big_stack)
+    if out.returncode != 0:
+        raise RuntimeError("vlinegen failed (%d):\n%s" % (out.returncode, out.stdout[-3000:]))
+    m = re.search(r"Wrote veto lines in band to: (\S+)", out.stdout)
+    with open(os.path.join(wd, m.group(1)), encoding="latin-1") as f:
+        return f.read()
 
 
 # ------------------------------------------------------------------ oracle

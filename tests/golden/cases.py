@@ -85,6 +85,23 @@ CASES = {
         narrowdown=0.45, veto_flag=1, line_files=LINE_FILES_100HZ,
         injections=(synth.Injection(f=100.035, fdot=-2e-10, ra=2.1, dec=-0.4, iota=0.7, psi=0.3,
                                     phase=1.1, snr=30.0),)),
+    # a three-detector network (H1, L1, V1: the general detector loop of the
+    # demodulation and the sky stage) with an injection
+    "g6_h1l1v1": synth.Case(
+        dt=8.0, nod=1, band=1440, dets=("H1", "L1", "V1"), sigma=(1.0, 1.2, 1.5), seed=88, thr=8.0,
+        fdot_step=2e-10, sky_cells=12.0,
+        gtype="allsky_range", gcenter=(100.031, -2e-10, 0.7, 0.9),
+        gsizes=(3600, 3.0, 1.0, 1.0), gsteps=(1, 1.0, 1.0, 1.0),
+        injections=(synth.Injection(f=100.031, fdot=-2e-10, ra=0.7, dec=0.9, iota=0.4, psi=1.2,
+                                    phase=2.0, snr=30.0),)),
+    # fftpad = 2 in the grid file: spindown FFTs of nfftf = 2 nfft and the
+    # F-statistic range scaled by it (settings.c:83-84)
+    "g7_fftpad2": synth.Case(
+        dt=16.0, nod=1, band=2880, dets=("H1",), seed=99, thr=7.0, fftpad=2,
+        gtype="directed_range", gcenter=(100.0152, -2e-10, 1.2, 0.3),
+        gsizes=(1800, 3.0, 0.0, 0.0), gsteps=(1, 1.0, 1.0, 1.0),
+        injections=(synth.Injection(f=100.0152, fdot=-2e-10, ra=1.2, dec=0.3, iota=0.2, psi=0.5,
+                                    phase=0.4, snr=25.0),)),
     # all-sky grid (spindown range from Smin/Smax per sky point, both
     # hemispheres) with blocks_avg F-statistic normalisation
     "g3_allsky_blocks": synth.Case(

@@ -258,8 +258,13 @@ struct HostPoint {
 struct tdf_engine {
      int dev = 0, form = TDF_FORM_SPLIT;
      cudaStream_t own = nullptr, stream = nullptr;
-     cudaStream_t sky_stream = nullptr;   // sky stage of the next batch runs here, overlapping
-     bool overlap = false;                // true: sky stage on its own stream (TDF_SKY_OVERLAP=1)
+     // The sky stage of the next batch runs on sky_stream, created at the
+     // lowest stream priority while the engine's own stream and the lanes
+     // get the highest: its CTAs take the SMs the spindown passes leave
+     // free in their tails instead of competing with them (TDF_SKY_OVERLAP=0:
+     // sky stage on the engine stream, serialised with the spindown stage).
+     cudaStream_t sky_stream = nullptr;
+     bool overlap = true;
      cudaEvent_t sky_done[2] = {nullptr, nullptr}, spin_done[2] = {nullptr, nullptr};
      tdf_segment seg{};
      tdf_search_opts opts{};
@@ -1278,7 +1283,7 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (tc && atoi(tc) > 0) e->Tc = atoi(tc);
      e->TcMax = std::max(48, e->Tc);
      const char *ov = getenv("TDF_SKY_OVERLAP");
-     e->overlap = ov && atoi(ov) != 0;   // measured: off is faster when the spindown kernels fill the GPU
+     if (ov && ov[0] == '0') e->overlap = false;
      const char *nl = getenv("TDF_LANES");
      if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
      const char *gr = getenv("TDF_GRAPHS");
@@ -1292,11 +1297,13 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      e->opts.lines = nullptr;
      e->dets.resize(seg->nifo);
      int st = TDF_OK;
-     cudaError_t ce = cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking);
-     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->sky_stream, cudaStreamNonBlocking);
+     int prio_low = 0, prio_high = 0;   // numerically: low >= high
+     cudaError_t ce = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+     if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->own, cudaStreamNonBlocking, prio_high);
+     if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->sky_stream, cudaStreamNonBlocking, prio_low);
      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
      for (int l = 1; l < e->nlanes && ce == cudaSuccess; l++) {
-          ce = cudaStreamCreateWithFlags(&e->lane_own[l], cudaStreamNonBlocking);
+          ce = cudaStreamCreateWithPriority(&e->lane_own[l], cudaStreamNonBlocking, prio_high);
           if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join_ev[l], cudaEventDisableTiming);
      }
      for (int k = 0; k < 2 && ce == cudaSuccess; k++) {

@@ -45,6 +45,29 @@ def test_graph_replay_matches_plain_launches(golden, monkeypatch, name):
     eng.close()
 
 
+@pytest.mark.parametrize("name", ["g2_h1l1_inj", "g6_h1l1v1"])
+def test_sky_stage_overlap_matches_in_line(golden, monkeypatch, name):
+    """The default runs the next batch's sky stage on its own low-priority
+    stream; TDF_SKY_OVERLAP=0 runs it in line on the engine stream.  Small
+    sky batches give several batches per search, so the overlap is used."""
+    from tdfstat_b200.engine import Engine
+    g = golden(name)
+    pm, mm, nn = g.job32.sky_points()
+    ref = None
+    for ov in ("0", None):
+        if ov is None:
+            monkeypatch.delenv("TDF_SKY_OVERLAP")
+        else:
+            monkeypatch.setenv("TDF_SKY_OVERLAP", ov)
+        eng = Engine(g.job32.segment(), g.job32.search_opts(), form="split", device=0, max_sky_batch=2)
+        got = _records(eng.search(pm, mm, nn))
+        eng.close()
+        if ref is None:
+            ref = got
+        else:
+            _same(got, ref)
+
+
 def test_records_do_not_depend_on_chunk_size(golden):
     from tdfstat_b200.engine import Engine, TdfError
     g = golden("g2_h1l1_inj")

@@ -743,11 +743,18 @@ static float rec_fdot(const tdf_engine *e, double spnd) {
 
 // ------------------------------------------------------------------ device pipeline
 
+// The stream of the sky stage: its own one when it overlaps the spindown
+// stage, the engine stream otherwise and while kernels are being timed (the
+// per-kernel event times are then those of kernels running alone).
+static cudaStream_t sky_stream_of(const tdf_engine *e) {
+     return e->overlap && !e->timing ? e->sky_stream : e->stream;
+}
+
 // Sky stage of npts points into batch slot e->cur, on the sky stream: it
 // first waits until the slot's previous spindown work released the slot's
 // operands, and records sky_done[slot] for the spindown work to wait on.
 static int run_sky_stage(tdf_engine *e, int npts) {
-     cudaStream_t st = e->overlap ? e->sky_stream : e->stream;
+     cudaStream_t st = sky_stream_of(e);
      CUCHK(cudaStreamWaitEvent(st, e->spin_done[e->cur], 0));
      const int nifo = e->nifo, Q = npts * nifo;
      const size_t ws = Wstride(e);
@@ -1129,7 +1136,7 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
                          q.id = (uint32_t)(P.first_tmpl + s);
                     }
                }
-               cudaStream_t sst = e->overlap ? e->sky_stream : e->stream;
+               cudaStream_t sst = sky_stream_of(e);
                size_t sev = e->timing ? timing_begin(e, sst) : (size_t)-1;
                TRY(run_sky_stage(e, nb));
                if (e->timing) timing_end(e, sev, KT_SKY, nb, sst);

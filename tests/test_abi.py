@@ -106,6 +106,25 @@ def test_invalid_arguments(lib):
     assert lib.tdf_status_string(_abi.TDF_ERR_TRIGGER_OVERFLOW) == b"too many triggers in one spindown"
 
 
+def test_frequency_range_below_bin_zero_is_refused(lib, tmp_path):
+    """A directed range whose frequency band starts below bin 0 makes the
+    reference write F before its array (jobcore.c:481-484 with fr[0] < 0,
+    heap corruption, seen here as an abort of the reference build); the
+    library refuses such a range before it touches a device."""
+    import dataclasses
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from golden.cases import CASES
+    from tdfstat_b200 import host, synth
+    case = dataclasses.replace(CASES["g6_h1l1v1"], gcenter=(100.027, -2e-10, 0.7, 0.9))
+    job = host.Job(synth.write_case(str(tmp_path), case))
+    assert job.range.fr[0] < 0
+    seg, opts = job.segment(), job.search_opts()
+    h = C.c_void_p()
+    assert lib.tdf_engine_create(C.byref(seg), C.byref(opts), 0, 0, 0, C.byref(h)) == _abi.TDF_ERR_INVALID
+    assert b"fr range" in lib.tdf_last_error()
+
+
 def test_engine_module_refuses_missing_library(tmp_path):
     from tdfstat_b200 import engine
     with pytest.raises(RuntimeError):

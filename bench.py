@@ -378,8 +378,17 @@ def run_tdf_segments(args, rank, world, local_rank):
     root = tempfile.mkdtemp(prefix="tdfbench4_")
     engines = {}
     try:
-        mw = MultiWorkload(root, world=world)
-        shards = [(w,) + tuple(w.shard(rank, world)) for w in mw.segments]
+        if args.segments_by_cost:
+            # whole segments to ranks by estimated cost; the total work is fixed
+            from tdfstat_b200 import shard as _shard
+            mw = MultiWorkload(root, world=1)
+            costs = [_shard.segment_cost(w.templates, w.job.sett.nfftf, w.job.sett.nifo, w.job.sett.N)
+                     for w in mw.segments]
+            mine = set(_shard.assign_segments(costs, world)[rank])
+            shards = [(w,) + tuple(w.shard(0, 1)) for k, w in enumerate(mw.segments) if k in mine]
+        else:
+            mw = MultiWorkload(root, world=world)
+            shards = [(w,) + tuple(w.shard(rank, world)) for w in mw.segments]
         stream = torch.cuda.Stream(device=local_rank)
         tuned = {}
         for w, pm, mm, nn in shards:
@@ -449,10 +458,13 @@ def run_tdf_segments(args, rank, world, local_rank):
         return {
             "metric": METRIC, "value": round(float(n[0]) / (ms / 1e3), 1), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong" if args.segments_by_cost else "weak",
+            "vs_baseline": None,
             "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
             "data": "synthetic (seeded Gaussian noise + injected CW signal per segment, synthetic ephemeris)",
             "config": dict(mw.config, form=args.form, templates_per_chunk={str(k): v for k, v in tuned.items()},
+                           distribution=("whole segments to ranks by estimated cost" if args.segments_by_cost
+                                         else "every segment's sky patch split over the ranks"),
                            templates_searched_per_step=int(round(float(n[0]) / args.steps)),
                            engines="one per segment size, segments streamed in by tdf_engine_upload each step",
                            l2="flush: 256 MiB write between timed steps; per-step working set > L2"),
@@ -512,6 +524,8 @@ def main():
     ap.add_argument("--sky-batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--segments-by-cost", action="store_true",
+                    help="cfg4 on several GPUs: whole segments to ranks by estimated cost (strong scaling)")
     ap.add_argument("--sky-points", type=int, default=0, help="use only the first K sky points (profiling runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

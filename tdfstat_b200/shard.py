@@ -46,6 +46,30 @@ def balanced_ranges(costs: Sequence[float], world: int) -> List[Tuple[int, int]]
     return out
 
 
+def segment_cost(templates: int, nfftf: int, nifo: int, N: int) -> float:
+    """Estimated device time of one segment's search: per template two FFTs
+    of nfftf (5 nfftf log2 nfftf flops each) and the demodulation of nifo*N
+    samples (about 40 flops each)."""
+    return float(templates) * (10.0 * nfftf * np.log2(nfftf) + 40.0 * nifo * N)
+
+
+def assign_segments(costs: Sequence[float], world: int) -> List[List[int]]:
+    """Whole segments to ranks (the reference runs one segment per process,
+    so a segment's records never need merging): longest first, each to the
+    rank with the least cost so far (ties: the lower rank); every rank's
+    list in segment order.  The most loaded rank carries at most
+    4/3 of the optimum (Graham's bound for this rule)."""
+    if world < 1:
+        raise ValueError("world %d" % world)
+    load = [0.0] * world
+    out: List[List[int]] = [[] for _ in range(world)]
+    for k in sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(k)
+        load[r] += float(costs[k])
+    return [sorted(x) for x in out]
+
+
 def merge_records(parts):
     """Concatenates per-rank (hdr, lens, pairs_flat) in rank order; returns
     the same triple for the whole run."""

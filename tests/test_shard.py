@@ -83,3 +83,57 @@ def test_two_rank_shards_merge_to_single_run(golden, oracle):
     np.testing.assert_array_equal(hdr, ref.hdr)
     np.testing.assert_array_equal(lens, [len(x) for x in ref.pairs])
     np.testing.assert_array_equal(flat, np.concatenate(ref.pairs))
+
+
+def test_assign_segments_partitions_and_balances():
+    rng = np.random.default_rng(3)
+    # the four segment sizes of the segmented workload, 64 segments, as costs
+    sizes = [(86164, 131072), (129246, 131072), (172328, 262144), (258492, 262144)]
+    costs = [shard.segment_cost(256 * 401, nf, 2, N) for N, nf in (sizes[k % 4] for k in range(64))]
+    for world in (1, 2, 3, 4, 8):
+        a = shard.assign_segments(costs, world)
+        assert sorted(k for r in a for k in r) == list(range(64))
+        assert all(r == sorted(r) for r in a)
+        loads = [sum(costs[k] for k in r) for r in a]
+        assert max(loads) <= 4.0 / 3.0 * max(sum(costs) / world, max(costs)) + 1e-6
+    rand = list(rng.uniform(1, 10, size=37))
+    a = shard.assign_segments(rand, 5)
+    loads = [sum(rand[k] for k in r) for r in a]
+    assert max(loads) - min(loads) <= max(rand)
+    assert shard.assign_segments([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        shard.assign_segments([1.0], 0)
+
+
+def _seg_worker(rank, world, port, costs, out_q):
+    import torch.distributed as dist
+    from tdfstat_b200 import shard as sh
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    mine = sh.assign_segments(costs, world)[rank]
+    every = [None] * world
+    dist.all_gather_object(every, mine)
+    if rank == 0:
+        out_q.put(every)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_take_disjoint_segments():
+    """Every rank computes the same assignment on its own (no exchange); the
+    ranks' segments are disjoint and cover all segments."""
+    import torch.multiprocessing as mp
+    costs = [shard.segment_cost(1000, 1 << (17 + (k % 2)), 2, 86164 * (1 + k % 3)) for k in range(11)]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_seg_worker, args=(r, 2, port, costs, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    every = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert sorted(every[0] + every[1]) == list(range(11))
+    assert not set(every[0]) & set(every[1])

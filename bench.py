@@ -389,7 +389,9 @@ def run_tdf_segments(args, rank, world, local_rank):
         else:
             mw = MultiWorkload(root, world=world)
             shards = [(w,) + tuple(w.shard(rank, world)) for w in mw.segments]
-        stream = torch.cuda.Stream(device=local_rank)
+        # above the default priority, so that the engines' low-priority sky
+        # stream fills this stream's kernel tails instead of competing
+        stream = torch.cuda.Stream(device=local_rank, priority=-1)
         tuned = {}
         for w, pm, mm, nn in shards:
             N = w.job.sett.N

@@ -274,7 +274,12 @@ int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, int32_t nifo
                               int32_t fr0, int32_t fr1, float *d_F, void *stream);
 
 /* The CUDA stream the engine enqueues on (a cudaStream_t), and a way to make
-   it enqueue on the caller's stream instead (NULL = the engine's own). */
+   it enqueue on the caller's stream instead (NULL = the engine's own, which
+   has the device's highest stream priority).  The sky stage of the next
+   batch runs on an internal stream of the lowest priority, overlapping the
+   spindown stage, only while the engine's stream has a higher priority than
+   that; on a caller's stream of the default (lowest) priority it runs in
+   line. */
 int tdf_engine_get_stream(tdf_engine *e, void **stream);
 int tdf_engine_set_stream(tdf_engine *e, void *stream);
 

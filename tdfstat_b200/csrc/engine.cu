@@ -265,6 +265,8 @@ struct tdf_engine {
      // sky stage on the engine stream, serialised with the spindown stage).
      cudaStream_t sky_stream = nullptr;
      bool overlap = true;
+     int prio_low = 0, prio_high = 0;     // the device's stream priority range (low >= high numerically)
+     bool stream_outranks_sky = true;     // the engine stream has a higher priority than sky_stream
      cudaEvent_t sky_done[2] = {nullptr, nullptr}, spin_done[2] = {nullptr, nullptr};
      tdf_segment seg{};
      tdf_search_opts opts{};
@@ -746,8 +748,11 @@ static float rec_fdot(const tdf_engine *e, double spnd) {
 // The stream of the sky stage: its own one when it overlaps the spindown
 // stage, the engine stream otherwise and while kernels are being timed (the
 // per-kernel event times are then those of kernels running alone).
+// A caller's stream of the lowest priority would compete with the sky
+// stream on equal terms, which measured slower than running the sky stage
+// in line, so the overlap then stays off.
 static cudaStream_t sky_stream_of(const tdf_engine *e) {
-     return e->overlap && !e->timing ? e->sky_stream : e->stream;
+     return e->overlap && !e->timing && e->stream_outranks_sky ? e->sky_stream : e->stream;
 }
 
 // Sky stage of npts points into batch slot e->cur, on the sky stream: it
@@ -1304,8 +1309,9 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      e->opts.lines = nullptr;
      e->dets.resize(seg->nifo);
      int st = TDF_OK;
-     int prio_low = 0, prio_high = 0;   // numerically: low >= high
+     int &prio_low = e->prio_low, &prio_high = e->prio_high;
      cudaError_t ce = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+     e->stream_outranks_sky = prio_high < prio_low;
      if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->own, cudaStreamNonBlocking, prio_high);
      if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->sky_stream, cudaStreamNonBlocking, prio_low);
      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
@@ -1601,6 +1607,9 @@ int tdf_engine_set_stream(tdf_engine *e, void *stream) {
      CUCHK(cudaSetDevice(e->dev));
      CUCHK(cudaStreamSynchronize(e->stream));
      e->stream = stream ? (cudaStream_t)stream : e->own;
+     int p = e->prio_low;
+     CUCHK(cudaStreamGetPriority(e->stream, &p));
+     e->stream_outranks_sky = p < e->prio_low;
      return TDF_OK;
 }
 

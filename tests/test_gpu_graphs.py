@@ -66,6 +66,15 @@ def test_sky_stage_overlap_matches_in_line(golden, monkeypatch, name):
             ref = got
         else:
             _same(got, ref)
+    # on a caller's stream: default priority (sky stage in line) and a
+    # higher one (sky stage overlapped)
+    import torch
+    for prio in (0, -1):
+        s = torch.cuda.Stream(device=0, priority=prio)
+        eng = Engine(g.job32.segment(), g.job32.search_opts(), form="split", device=0, max_sky_batch=2)
+        eng.set_stream(s.cuda_stream)
+        _same(_records(eng.search(pm, mm, nn)), ref)
+        eng.close()
 
 
 def test_records_do_not_depend_on_chunk_size(golden):

@@ -27,8 +27,9 @@ from .shard import shard_points
 
 def workload_case(name: str):
     if name == "cfg1":
+        # directed_range gives 2g+1 spindowns: 65 for the 64 of the reference's single-point case
         return synth.Case(dt=2.0, nod=2, band=360, dets=("H1",), read_o3=True, seed=101, thr=14.5,
-                          fdot_step=1e-10, sky_cells=16.0), (1, 1), 64, 0.25
+                          fdot_step=1e-10, sky_cells=16.0), (1, 1), 65, 0.25
     if name == "cfg5":
         inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
         return synth.Case(dt=2.0, nod=6, band=360, dets=("H1", "L1"), sigma=(1.0, 1.3), gap_frac=0.10, seed=505,

@@ -1,11 +1,12 @@
-"""Parity at the benchmark sizes: cfg2 (N = 86164, nfftf = 2^17) and cfg3
+"""Parity at the benchmark sizes: cfg1 (H1 alone, float64 input read as
+mods=read_O3, N = 86164), cfg2 (H1L1, N = 86164, nfftf = 2^17) and cfg3
 (N = 258492, nfftf = 2^18), through checks the FP64 oracle finishes in
 seconds:
   * F spectra of single templates (first and last spindown of two sky points)
     against orc_fstat_spectrum,
   * the records of one sky point x 21 spindowns against orc_search_points,
-  * the injected signal is the loudest trigger over all 401 spindowns of the
-    sky point nearest to it.
+  * the injected signal (cfg2, cfg3) is the loudest trigger over all 401
+    spindowns of the sky point nearest to it.
 Tolerances as in test_gpu_parity: FP64 form 1e-10, split form 1e-4
 (normalised F error), identical triggers up to threshold/neighbour ties.
 """
@@ -51,7 +52,7 @@ def _job(wl, j64, form):
 
 
 @pytest.mark.parametrize("form", ["split", "fp64"])
-@pytest.mark.parametrize("name", ["cfg2", "cfg3"])
+@pytest.mark.parametrize("name", ["cfg1", "cfg2", "cfg3"])
 def test_fullsize_spectrum_matches_oracle(workload, oracle, name, form):
     wl, j64 = workload(name)
     seg, opts = j64.segment(), j64.search_opts()
@@ -73,7 +74,7 @@ def test_fullsize_spectrum_matches_oracle(workload, oracle, name, form):
 
 
 @pytest.mark.parametrize("form", ["split", "fp64"])
-@pytest.mark.parametrize("name", ["cfg2", "cfg3"])
+@pytest.mark.parametrize("name", ["cfg1", "cfg2", "cfg3"])
 def test_fullsize_records_match_oracle(workload, oracle, name, form):
     wl, j64 = workload(name)
     seg, opts = j64.segment(), j64.search_opts()

@@ -93,9 +93,18 @@ class Engine:
         self.nF = opts.fr[1] - opts.fr[0] + 1
 
     @classmethod
-    def from_job(cls, job, form: str = "split", device: int = 0, max_sky_batch: int = 0) -> "Engine":
+    def from_job(cls, job, form: Optional[str] = None, device: Optional[int] = None,
+                 max_sky_batch: Optional[int] = None) -> "Engine":
+        """An engine for a host.Job; arguments left out come from the job's
+        INI [gpu] section (host.GpuOptions), else split form on device 0."""
+        g = getattr(job, "gpu", None)
+        form = form if form is not None else (g.form if g else "split")
+        device = device if device is not None else (g.device if g else 0)
+        max_sky_batch = max_sky_batch if max_sky_batch is not None else (g.sky_batch if g else 0)
         e = cls(job.segment(), job.search_opts(), form=form, device=device, max_sky_batch=max_sky_batch)
         e.job = job
+        if g and g.templates_per_chunk:
+            e.templates_per_chunk = g.templates_per_chunk
         return e
 
     def close(self):

@@ -497,6 +497,34 @@ def sky_points(rng: SearchRange):
     return pms, mms, nns
 
 
+# ---------------------------------------------------------------- [gpu] section
+
+@dataclass
+class GpuOptions:
+    """The INI's [gpu] section, read by this library only (the reference's
+    iniparser-based host ignores sections it does not ask for):
+    form = split | fp64, device = CUDA device, sky_batch = sky points per
+    batch (0: the library's default), templates_per_chunk = templates per
+    pass launch (0: the library's default, or what tdf_engine_autotune
+    picks)."""
+    form: str = "split"
+    device: int = 0
+    sky_batch: int = 0
+    templates_per_chunk: int = 0
+
+
+def gpu_options(ini: Dict[str, str]) -> GpuOptions:
+    g = GpuOptions(form=(ini.get("gpu:form", "") or "split").lower(),
+                   device=int(ini.get("gpu:device", "") or 0),
+                   sky_batch=int(ini.get("gpu:sky_batch", "") or 0),
+                   templates_per_chunk=int(ini.get("gpu:templates_per_chunk", "") or 0))
+    if g.form not in ("split", "fp64"):
+        raise ValueError("[gpu] form must be split or fp64, not %r" % g.form)
+    if g.device < 0 or g.sky_batch < 0 or not (0 <= g.templates_per_chunk <= 48):
+        raise ValueError("[gpu] device/sky_batch >= 0 and templates_per_chunk in 0..48")
+    return g
+
+
 # ---------------------------------------------------------------- veto lines
 # narrow_down_band, read_band_vlines, extract_band_vlines: tdfstat_b200/vlines.py
 
@@ -560,6 +588,7 @@ class Job:
         self.mods = ini.get("search:mods", "")
         self.fstat_norm = ini.get("search:fstat_norm", "")
         self.veto_flag = int(ini.get("search:veto_flag", "0") or 0)
+        self.gpu = gpu_options(ini)
         self.gtype = ini.get("grid:gtype", "allsky")
         outdir = ini.get("search:outdir", ".")
         if not os.path.isabs(outdir):

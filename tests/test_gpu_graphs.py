@@ -107,3 +107,24 @@ def test_tma_staged_operands_match(golden, monkeypatch, name):
     eng = Engine.from_job(g.job32, form="split")
     _same(_records(eng.search(pm, mm, nn)), ref)
     eng.close()
+
+
+def test_engine_takes_the_ini_gpu_section(golden):
+    """Engine.from_job without arguments uses the job's [gpu] options."""
+    import dataclasses
+    from tdfstat_b200 import host
+    from tdfstat_b200.engine import Engine
+    g = golden("g2_h1l1_inj")
+    job = g.job32
+    keep = job.gpu
+    try:
+        job.gpu = dataclasses.replace(host.GpuOptions(), form="fp64", templates_per_chunk=3)
+        eng = Engine.from_job(job)
+        assert eng.form == "fp64" and eng.templates_per_chunk == 3
+        eng.close()
+        job.gpu = host.GpuOptions()
+        eng = Engine.from_job(job)
+        assert eng.form == "split"
+        eng.close()
+    finally:
+        job.gpu = keep

@@ -332,7 +332,7 @@ def run_tdf(args, rank, world, local_rank):
                         "timed": "CUDA events on the engine stream around each launch, one lane, %d templates "
                                  "per launch (the run itself: %d per chunk over concurrent lanes)" % (tc_timed, tc_run)}
             cpu = None
-            if not args.no_cpu_baseline:
+            if not args.no_cpu_baseline and world == 1:   # the CPU baseline is an N = 1 figure
                 r = cpu_reference_sample(wl, tempfile.mkdtemp(prefix="tdfcpu_"), 3, os.cpu_count() or 1)
                 if r:
                     nrec_c, secs = r

@@ -8,10 +8,18 @@
 // Every expression keeps the reference's float/double evaluation (its build,
 // coincidences/Makefile, contracts f + a*b into one fused multiply-add,
 // which the segment shift below reproduces with std::fma).
+//
+// The 16 cell shifts are independent searches over the same selected
+// triggers: they run on up to 16 host threads (TDF_COINC_THREADS, default
+// the hardware threads), each with its own scratch, and their results are
+// joined in shift order, so the output does not depend on the thread count.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <thread>
 #include <vector>
 
 #include "tdfcuda.h"
@@ -69,8 +77,142 @@ struct CellState {     // per (segment, frequency cell) of the current (m, n, s)
 struct Coi {
      float avg_snr, avg_f, avg_fdot, avg_ra, avg_dec;
      int w;
-     int64_t member;
+     int64_t member;   // first member in the result's member arrays
 };
+
+struct ShiftInput {
+     const tdf_coinc_opts *o;
+     int nseg;
+     const tdf_record *hdr;   // ctrigs take segment 0's headers (coincidences.c:80-91)
+     int64_t nrec;
+     int nfc;                 // frequency cells
+     int nfftf;
+     const std::vector<std::vector<int64_t>> *off;
+     const std::vector<std::vector<Good>> *good;
+};
+
+struct ShiftScratch {
+     struct Key { int mc, nc, sc; };
+     std::vector<CellState> st;
+     std::vector<int> dirty, fics;
+     std::vector<int32_t> order;
+     std::vector<Key> key;
+};
+
+struct ShiftResult {
+     std::vector<Coi> coi;                  // in output order
+     std::vector<int16_t> mem_seg, mem_n;
+     std::vector<int32_t> mem_trig;
+     std::vector<int32_t> uniq;             // per segment: coincidence members
+};
+
+// One cell shift ish (bits m, n, s, f = 8, 4, 2, 1): coincidences.c:196-367.
+static void run_shift(const ShiftInput &in, int ish, ShiftScratch &sc, ShiftResult &r) {
+     const tdf_coinc_opts *o = in.o;
+     const int nseg = in.nseg, nfc = in.nfc, nfftf = in.nfftf;
+     const int64_t nrec = in.nrec;
+     const tdf_record *hdr = in.hdr;
+     const auto &off = *in.off;
+     const auto &good = *in.good;
+     sc.st.assign((size_t)nseg * nfc, CellState());
+     sc.order.resize(nrec);
+     sc.key.resize(nrec);
+     auto &st = sc.st;
+     auto &order = sc.order;
+     auto &key = sc.key;
+     auto &dirty = sc.dirty;
+     auto &fics = sc.fics;
+     r.coi.clear();
+     r.mem_seg.clear();
+     r.mem_n.clear();
+     r.mem_trig.clear();
+     r.uniq.assign(nseg, 0);
+     int32_t *un = r.uniq.data();
+     auto &mem_seg = r.mem_seg;
+     auto &mem_trig = r.mem_trig;
+     auto &mem_n = r.mem_n;
+     auto &shift_coi = r.coi;
+     const float shm = ((ish >> 3) & 1) * 0.5f, shn = ((ish >> 2) & 1) * 0.5f;
+     const float shs = ((ish >> 1) & 1) * 0.5f, shf = (ish & 1) * 0.5f;
+     for (int64_t j = 0; j < nrec; j++) {
+          key[j].mc = (int)floorf(hdr[j].m / o->scalem - shm);
+          key[j].nc = (int)floorf(hdr[j].n / o->scalen - shn);
+          key[j].sc = (int)floorf(hdr[j].s / o->scales - shs);
+          order[j] = (int32_t)j;
+     }
+     // the reference's qsort (glibc: a merge sort, stable) by (mc, nc, sc)
+     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+          if (key[a].mc != key[b].mc) return key[a].mc < key[b].mc;
+          if (key[a].nc != key[b].nc) return key[a].nc < key[b].nc;
+          return key[a].sc < key[b].sc;
+     });
+     for (int64_t c0 = 0; c0 < nrec;) {
+          int64_t c1 = c0 + 1;
+          while (c1 < nrec && key[order[c1]].mc == key[order[c0]].mc && key[order[c1]].nc == key[order[c0]].nc &&
+                 key[order[c1]].sc == key[order[c0]].sc)
+               c1++;
+          // pass 1 (:264-294): the loudest trigger per (segment, frequency cell)
+          dirty.clear();
+          for (int64_t jj = c0; jj < c1; jj++) {
+               const int32_t cidx = order[jj];
+               for (int s = 0; s < nseg; s++) {
+                    for (int64_t k = off[s][cidx]; k < off[s][cidx + 1]; k++) {
+                         const float f = good[s][k].f;
+                         const float snr2 = (float)(2. * good[s][k].F - 4.);
+                         const int fic = (int)floorf((float)((double)f / (M_PI / nfftf) / o->scalef - shf));
+                         if ((unsigned)fic >= (unsigned)nfc) continue;
+                         CellState &cs = st[(size_t)s * nfc + fic];
+                         if (cs.best < 0 && cs.ntrig == 0) dirty.push_back(s * nfc + fic);
+                         cs.ntrig++;
+                         if (snr2 > cs.best_snr) {
+                              cs.best_snr = snr2;
+                              cs.best = cidx;
+                              cs.best_f = f;
+                         }
+                    }
+               }
+          }
+          // pass 2 (:296-362), over the frequency cells touched, increasing
+          fics.clear();
+          for (int d : dirty) fics.push_back(d % nfc);
+          std::sort(fics.begin(), fics.end());
+          fics.erase(std::unique(fics.begin(), fics.end()), fics.end());
+          for (int fic : fics) {
+               int w = 0;
+               float sum_snr = 0.f, sum_f = 0.f, sum_fdot = 0.f, sum_ra = 0.f, sum_dec = 0.f;
+               const size_t m0 = mem_seg.size();
+               for (int s = 0; s < nseg; s++) {
+                    const CellState &cs = st[(size_t)s * nfc + fic];
+                    if (cs.best < 0) continue;
+                    un[s]++;
+                    mem_seg.push_back((int16_t)s);
+                    mem_trig.push_back(cs.best);
+                    mem_n.push_back(cs.ntrig);
+                    sum_snr += cs.best_snr;
+                    sum_f += cs.best_f;
+                    sum_fdot += hdr[cs.best].fdot;
+                    sum_ra += hdr[cs.best].ra;
+                    sum_dec += hdr[cs.best].dec;
+                    w++;
+               }
+               if (w < o->mincoin) {
+                    mem_seg.resize(m0);
+                    mem_trig.resize(m0);
+                    mem_n.resize(m0);
+                    continue;
+               }
+               shift_coi.push_back(Coi{sqrtf(sum_snr / w), sum_f / w, sum_fdot / w, sum_ra / w, sum_dec / w, w,
+                                       (int64_t)m0});
+          }
+          for (int d : dirty) st[d] = CellState();
+          c0 = c1;
+     }
+     // qsort(coi, cmp_coi) (:365): more segments first, then higher SNR; stable
+     std::stable_sort(shift_coi.begin(), shift_coi.end(), [](const Coi &a, const Coi &b) {
+          if (a.w != b.w) return a.w > b.w;
+          return a.avg_snr > b.avg_snr;
+     });
+}
 
 }  // namespace
 
@@ -99,110 +241,56 @@ extern "C" int tdf_coincidences(const tdf_coinc_opts *o, int32_t nseg, const tdf
      std::vector<std::vector<Good>> good(nseg);
      std::vector<int32_t> nsel(nseg);
      for (int s = 0; s < nseg; s++) nsel[s] = (int32_t)select_good(*o, segs[s], off[s], good[s]);
-     const tdf_record *hdr = segs[0].recs;   // ctrigs take segment 0's headers (coincidences.c:80-91)
-     const int nfc = nfftf / o->scalef;      // frequency cells
      const int ish0 = o->shift < 0 ? 0 : o->shift, ish1 = o->shift < 0 ? 15 : o->shift;
-     std::vector<CellState> st((size_t)nseg * nfc);
-     std::vector<int> dirty;
-     std::vector<int> fics;
-     std::vector<int32_t> order(nrec);
-     struct Key { int mc, nc, sc; };
-     std::vector<Key> key(nrec);
-     std::vector<Coi> all, shift_coi;
+     const int nsh = ish1 - ish0 + 1;
+     std::vector<ShiftResult> res(nsh);
+     const ShiftInput in{o, nseg, segs[0].recs, nrec, nfftf / o->scalef, nfftf, &off, &good};
+     int nthr = (int)std::thread::hardware_concurrency();
+     if (const char *ev = getenv("TDF_COINC_THREADS")) nthr = atoi(ev);
+     nthr = std::max(1, std::min(nthr, nsh));
+     std::vector<std::exception_ptr> fail(nthr);
+     auto work = [&](int t) {
+          try {
+               ShiftScratch sc;
+               for (int i = t; i < nsh; i += nthr) run_shift(in, ish0 + i, sc, res[i]);
+          } catch (...) {
+               fail[t] = std::current_exception();
+          }
+     };
+     {
+          // workers 1.. on threads (a worker whose thread cannot be started
+          // runs here instead), worker 0 on this thread
+          std::vector<std::thread> pool;
+          std::vector<int> inline_workers;
+          for (int t = 1; t < nthr; t++) {
+               try {
+                    pool.emplace_back(work, t);
+               } catch (...) {
+                    inline_workers.push_back(t);
+               }
+          }
+          work(0);
+          for (int t : inline_workers) work(t);
+          for (auto &th : pool) th.join();
+     }
+     for (auto &f : fail)
+          if (f) return tdf_internal_set_error(TDF_ERR_OUT_OF_MEMORY, "coincidence search: host allocation failed");
+     // join in shift order
+     std::vector<Coi> all;
+     std::vector<int32_t> shifts;
      std::vector<int16_t> mem_seg, mem_n;
      std::vector<int32_t> mem_trig;
-     std::vector<int32_t> shifts;
-     std::vector<int64_t> shift_begin;
-     std::vector<int32_t> uniq((size_t)(ish1 - ish0 + 1) * nseg, 0);
-     for (int ish = ish0; ish <= ish1; ish++) {
-          const float shm = ((ish >> 3) & 1) * 0.5f, shn = ((ish >> 2) & 1) * 0.5f;
-          const float shs = ((ish >> 1) & 1) * 0.5f, shf = (ish & 1) * 0.5f;
-          for (int64_t j = 0; j < nrec; j++) {
-               key[j].mc = (int)floorf(hdr[j].m / o->scalem - shm);
-               key[j].nc = (int)floorf(hdr[j].n / o->scalen - shn);
-               key[j].sc = (int)floorf(hdr[j].s / o->scales - shs);
-               order[j] = (int32_t)j;
-          }
-          // the reference's qsort (glibc: a merge sort, stable) by (mc, nc, sc)
-          std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-               if (key[a].mc != key[b].mc) return key[a].mc < key[b].mc;
-               if (key[a].nc != key[b].nc) return key[a].nc < key[b].nc;
-               return key[a].sc < key[b].sc;
-          });
-          shift_coi.clear();
-          const size_t mem0 = mem_seg.size();
-          int32_t *un = &uniq[(size_t)(ish - ish0) * nseg];
-          for (int64_t c0 = 0; c0 < nrec;) {
-               int64_t c1 = c0 + 1;
-               while (c1 < nrec && key[order[c1]].mc == key[order[c0]].mc && key[order[c1]].nc == key[order[c0]].nc &&
-                      key[order[c1]].sc == key[order[c0]].sc)
-                    c1++;
-               // pass 1 (:264-294): the loudest trigger per (segment, frequency cell)
-               dirty.clear();
-               for (int64_t jj = c0; jj < c1; jj++) {
-                    const int32_t cidx = order[jj];
-                    for (int s = 0; s < nseg; s++) {
-                         for (int64_t k = off[s][cidx]; k < off[s][cidx + 1]; k++) {
-                              const float f = good[s][k].f;
-                              const float snr2 = (float)(2. * good[s][k].F - 4.);
-                              const int fic = (int)floorf((float)((double)f / (M_PI / nfftf) / o->scalef - shf));
-                              if ((unsigned)fic >= (unsigned)nfc) continue;
-                              CellState &cs = st[(size_t)s * nfc + fic];
-                              if (cs.best < 0 && cs.ntrig == 0) dirty.push_back(s * nfc + fic);
-                              cs.ntrig++;
-                              if (snr2 > cs.best_snr) {
-                                   cs.best_snr = snr2;
-                                   cs.best = cidx;
-                                   cs.best_f = f;
-                              }
-                         }
-                    }
+     for (int i = 0; i < nsh; i++) {
+          for (Coi c : res[i].coi) {
+               const int64_t m0 = (int64_t)mem_seg.size();
+               for (int k = 0; k < c.w; k++) {
+                    mem_seg.push_back(res[i].mem_seg[c.member + k]);
+                    mem_trig.push_back(res[i].mem_trig[c.member + k]);
+                    mem_n.push_back(res[i].mem_n[c.member + k]);
                }
-               // pass 2 (:296-362), over the frequency cells touched, increasing
-               fics.clear();
-               for (int d : dirty) fics.push_back(d % nfc);
-               std::sort(fics.begin(), fics.end());
-               fics.erase(std::unique(fics.begin(), fics.end()), fics.end());
-               for (int fic : fics) {
-                    int w = 0;
-                    float sum_snr = 0.f, sum_f = 0.f, sum_fdot = 0.f, sum_ra = 0.f, sum_dec = 0.f;
-                    const size_t m0 = mem_seg.size();
-                    for (int s = 0; s < nseg; s++) {
-                         const CellState &cs = st[(size_t)s * nfc + fic];
-                         if (cs.best < 0) continue;
-                         un[s]++;
-                         mem_seg.push_back((int16_t)s);
-                         mem_trig.push_back(cs.best);
-                         mem_n.push_back(cs.ntrig);
-                         sum_snr += cs.best_snr;
-                         sum_f += cs.best_f;
-                         sum_fdot += hdr[cs.best].fdot;
-                         sum_ra += hdr[cs.best].ra;
-                         sum_dec += hdr[cs.best].dec;
-                         w++;
-                    }
-                    if (w < o->mincoin) {
-                         mem_seg.resize(m0);
-                         mem_trig.resize(m0);
-                         mem_n.resize(m0);
-                         continue;
-                    }
-                    shift_coi.push_back(Coi{sqrtf(sum_snr / w), sum_f / w, sum_fdot / w, sum_ra / w, sum_dec / w, w,
-                                            (int64_t)m0});
-               }
-               for (int d : dirty) st[d] = CellState();
-               c0 = c1;
-          }
-          // qsort(coi, cmp_coi) (:365): more segments first, then higher SNR; stable
-          std::stable_sort(shift_coi.begin(), shift_coi.end(), [](const Coi &a, const Coi &b) {
-               if (a.w != b.w) return a.w > b.w;
-               return a.avg_snr > b.avg_snr;
-          });
-          (void)mem0;
-          shift_begin.push_back((int64_t)all.size());
-          for (const Coi &c : shift_coi) {
+               c.member = m0;
                all.push_back(c);
-               shifts.push_back(ish);
+               shifts.push_back(ish0 + i);
           }
      }
      int64_t nm = 0;
@@ -215,7 +303,7 @@ extern "C" int tdf_coincidences(const tdf_coinc_opts *o, int32_t nseg, const tdf
                     int32_t *si = seginfo + ((size_t)(ish - ish0) * nseg + s) * 3;
                     si[0] = segs[s].seg;
                     si[1] = nsel[s];
-                    si[2] = uniq[(size_t)(ish - ish0) * nseg + s];
+                    si[2] = res[ish - ish0].uniq[s];
                }
      }
      if ((int64_t)all.size() > max_coi || nm > max_members)

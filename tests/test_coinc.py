@@ -82,8 +82,15 @@ def test_inputs_regenerate_identically(c1):
     assert c1.checksum == str(c1.fix["checksum"])
 
 
+@pytest.mark.parametrize("threads", ["1", "3", None])
 @pytest.mark.parametrize("key", ["a", "b"])
-def test_coincidences_match_reference_bit_for_bit(c1, oracle, key):
+def test_coincidences_match_reference_bit_for_bit(c1, oracle, key, threads, monkeypatch):
+    """The 16 shifts run on TDF_COINC_THREADS host threads (default: all);
+    the result is the reference's for any thread count."""
+    if threads is None:
+        monkeypatch.delenv("TDF_COINC_THREADS", raising=False)
+    else:
+        monkeypatch.setenv("TDF_COINC_THREADS", threads)
     segs = []
     for seg, _ in c1.segs:
         job = c1.jobs[seg]

@@ -128,3 +128,19 @@ def test_engine_takes_the_ini_gpu_section(golden):
         eng.close()
     finally:
         job.gpu = keep
+
+
+@pytest.mark.parametrize("name", ["g2_h1l1_inj", "g7_fftpad2"])
+def test_row_pass_without_bulk_copies_matches(golden, monkeypatch, name):
+    """TDF_ROW_BULK=0 (row-pass inputs by per-thread loads) gives the same
+    records as the default bulk copies into shared memory."""
+    from tdfstat_b200.engine import Engine
+    g = golden(name)
+    pm, mm, nn = g.job32.sky_points()
+    eng = Engine.from_job(g.job32, form="split")
+    ref = _records(eng.search(pm, mm, nn))
+    eng.close()
+    monkeypatch.setenv("TDF_ROW_BULK", "0")
+    eng = Engine.from_job(g.job32, form="split")
+    _same(_records(eng.search(pm, mm, nn)), ref)
+    eng.close()

@@ -107,6 +107,16 @@ typedef struct tdf_record {
 
 typedef struct tdf_engine tdf_engine;
 
+/* Bit set in a kernel's error word when a bounded wait on an asynchronous
+   copy gave up (the search then returns TDF_ERR_CUDA with a message). */
+#define TDF_WAIT_TIMEOUT_BIT 2u
+
+/* Health check of the bounded waits: one warp on `device` waits, `probes`
+   probes at most (1..2^20), on a barrier whose copy never arrives, and
+   returns; *status receives the kernel's error word (TDF_WAIT_TIMEOUT_BIT
+   set when the wait gave up, as it must).  The device stays usable. */
+int tdf_check_bounded_wait(int device, int32_t probes, uint32_t *status);
+
 const char *tdf_status_string(int status);
 /* message of the calling thread's last failed call ("" if none) */
 const char *tdf_last_error(void);

@@ -1225,9 +1225,51 @@ static void autotune_cache_store(const tdf_engine *e) {
      fclose(f);
 }
 
+// One warp waits on an mbarrier that announces 16 bytes of transactions no
+// copy will deliver: the bounded wait of the pipeline kernels gives up after
+// `probes` probes and the kernel reports ERR_STAGE_TIMEOUT, as a pass whose
+// bulk copies never completed would.  No copy is issued, so nothing is in
+// flight when the kernel returns.
+__global__ void k_wait_probe(unsigned *err, int probes) {
+     __shared__ __align__(8) uint64_t bar;
+     if (threadIdx.x == 0) {
+          mbar_init(&bar, 1);
+          mbar_fence_init();
+     }
+     __syncthreads();
+     if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);
+     const bool done = mbar_wait(&bar, 0u, probes);
+     if (!done && threadIdx.x == 0) atomicOr(err, ERR_STAGE_TIMEOUT);
+}
+
 // ------------------------------------------------------------------ C ABI
 
 extern "C" {
+
+int tdf_check_bounded_wait(int device, int32_t probes, uint32_t *status) {
+     if (!status || probes < 1 || probes > (1 << 20))
+          return set_error(TDF_ERR_INVALID, "status must be non-null and probes in 1..2^20");
+     int ndev = 0;
+     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+          cudaGetLastError();
+          return set_error(TDF_ERR_NO_DEVICE, "no CUDA device");
+     }
+     if (device < 0 || device >= ndev) return set_error(TDF_ERR_INVALID, "device %d of %d", device, ndev);
+     CUCHK(cudaSetDevice(device));
+     unsigned *d = nullptr;
+     CUCHK(cudaMalloc((void **)&d, sizeof(unsigned)));
+     cudaError_t ce = cudaMemset(d, 0, sizeof(unsigned));
+     if (ce == cudaSuccess) {
+          k_wait_probe<<<1, 32>>>(d, probes);
+          ce = cudaGetLastError();
+     }
+     unsigned h = 0;
+     if (ce == cudaSuccess) ce = cudaMemcpy(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost);
+     cudaFree(d);
+     if (ce != cudaSuccess) return set_error(TDF_ERR_CUDA, "bounded-wait check: %s", cudaGetErrorString(ce));
+     *status = h;
+     return TDF_OK;
+}
 
 const char *tdf_status_string(int status) {
      switch (status) {

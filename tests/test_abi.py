@@ -104,6 +104,10 @@ def test_invalid_arguments(lib):
     opts = _abi.TdfSearchOpts()
     assert lib.tdf_engine_create(C.byref(seg), C.byref(opts), 0, 0, 0, C.byref(h)) == _abi.TDF_ERR_INVALID
     assert lib.tdf_status_string(_abi.TDF_ERR_TRIGGER_OVERFLOW) == b"too many triggers in one spindown"
+    st = C.c_uint32(0)
+    assert lib.tdf_check_bounded_wait(0, 0, C.byref(st)) == _abi.TDF_ERR_INVALID
+    assert lib.tdf_check_bounded_wait(0, 1000, None) == _abi.TDF_ERR_INVALID
+    assert lib.tdf_check_bounded_wait(0, 1000, C.byref(st)) == _abi.TDF_ERR_NO_DEVICE
 
 
 def test_frequency_range_below_bin_zero_is_refused(lib, tmp_path):

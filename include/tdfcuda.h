@@ -200,6 +200,12 @@ typedef struct tdf_signal {
    tdf_engine_upload() replaces the data, injection included. */
 int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0, int32_t *in_band);
 
+/* h0*s_n[i], i < N, of the signal the last tdf_engine_add_signal() added to
+   detector `det` (n >= N values): what the reference writes with
+   mods=write_signal (init.c:475-497).  Held until the next search or upload
+   (the engine reuses the memory); TDF_ERR_INVALID when no signal is held. */
+int tdf_engine_get_signal(tdf_engine *e, int32_t det, double *out, int64_t n);
+
 /* Copies detector det's resident xDat (the first n <= N floats, injections
    included) to the host. */
 int tdf_engine_get_xdat(tdf_engine *e, int32_t det, float *xdat, int64_t n);

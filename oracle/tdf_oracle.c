@@ -62,6 +62,13 @@ void orc_modvir(const tdf_segment *seg, int det, double sinal, double cosal,
    init.c:462-464).  Expressions in the reference's evaluation order. */
 int orc_add_signal(const tdf_segment *seg, const tdf_signal *sig, double *h0_out)
 {
+     return orc_add_signal_out(seg, sig, h0_out, NULL);
+}
+
+/* the same, and h0*s_n[i] into signal_out[n*N + i] when it is not NULL: what
+   the reference writes with mods=write_signal (init.c:475-497) */
+int orc_add_signal_out(const tdf_segment *seg, const tdf_signal *sig, double *h0_out, double *signal_out)
+{
      const int N = seg->N, nifo = seg->nifo;
      const int dseg = sig->seg - sig->reffr;
      double freqo0 = 2 * M_PI * sig->freq * seg->dt;
@@ -107,6 +114,8 @@ int orc_add_signal(const tdf_segment *seg, const tdf_signal *sig, double *h0_out
           for (int i = 0; i < N; i++)
                if (x[i]) x[i] += h0 * s[(size_t)n * N + i];                   /* init.c:468-473 */
      }
+     if (signal_out)
+          for (size_t k = 0; k < (size_t)nifo * N; k++) signal_out[k] = h0 * s[k];   /* init.c:491 */
      free(s);
      free(aa);
      free(bb);

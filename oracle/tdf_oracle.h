@@ -53,6 +53,8 @@ void orc_splintpad(const double complex *ya, const double *shftf, int N,
    Returns 1 if the signal lies outside [fpo, fpo + B] (nothing added),
    else 0; *h0 receives the amplitude used. */
 int orc_add_signal(const tdf_segment *seg, const tdf_signal *sig, double *h0);
+/* the same, and h0*s_n[i] into signal_out[n*N + i] (if not NULL) */
+int orc_add_signal_out(const tdf_segment *seg, const tdf_signal *sig, double *h0, double *signal_out);
 
 /* textbook FFT (fft_core.c), exposed for the FFT tests */
 int orc_fft(int n, int sign, const double complex *in, double complex *out);

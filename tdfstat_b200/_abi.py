@@ -185,6 +185,7 @@ ABI_FUNCTIONS = [
     ("tdf_fstat_spectrum", C.c_int,
      [P, C.c_int32, C.c_float, C.c_float, C.c_float, F64P, C.c_int64]),
     ("tdf_engine_add_signal", C.c_int, [P, C.POINTER(TdfSignal), F64P, I32P]),
+    ("tdf_engine_get_signal", C.c_int, [P, C.c_int32, F64P, C.c_int64]),
     ("tdf_engine_get_xdat", C.c_int, [P, C.c_int32, F32P, C.c_int64]),
     ("tdf_coincidences", C.c_int,
      [C.POINTER(TdfCoincOpts), C.c_int32, C.POINTER(TdfCoincSegment), C.POINTER(TdfCoincidence), C.c_int64, I64P,

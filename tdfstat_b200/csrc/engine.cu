@@ -265,6 +265,10 @@ struct tdf_engine {
      // sky stage on the engine stream, serialised with the spindown stage).
      cudaStream_t sky_stream = nullptr;
      bool overlap = true;
+     // the last injected signal s_n[i] (tdf_engine_add_signal) stays in the
+     // sky work buffer B0 until the next sky stage or upload overwrites it
+     double signal_h0 = 0.;
+     bool signal_valid = false;
      int prio_low = 0, prio_high = 0;     // the device's stream priority range (low >= high numerically)
      bool stream_outranks_sky = true;     // the engine stream has a higher priority than sky_stream
      cudaEvent_t sky_done[2] = {nullptr, nullptr}, spin_done[2] = {nullptr, nullptr};
@@ -759,6 +763,7 @@ static cudaStream_t sky_stream_of(const tdf_engine *e) {
 // first waits until the slot's previous spindown work released the slot's
 // operands, and records sky_done[slot] for the spindown work to wait on.
 static int run_sky_stage(tdf_engine *e, int npts) {
+     e->signal_valid = false;   // B0 is the sky stage's work buffer
      cudaStream_t st = sky_stream_of(e);
      CUCHK(cudaStreamWaitEvent(st, e->spin_done[e->cur], 0));
      const int nifo = e->nifo, Q = npts * nifo;
@@ -1387,6 +1392,7 @@ int tdf_engine_upload(tdf_engine *e, const tdf_segment *seg) {
      tdf_search_opts o = e->opts;
      o.lines = e->lines.data();
      TRY(validate(seg, &o));
+     e->signal_valid = false;
      if (seg->N != e->N || seg->nfft != e->nfft || seg->nfftf != e->nfftf || seg->Ninterp != e->Ninterp ||
          seg->nifo != e->nifo)
           return set_error(TDF_ERR_INVALID, "segment sizes differ from the engine's");
@@ -1526,6 +1532,7 @@ int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0_out, 
      double freqo0 = 2 * M_PI * sig->freq * dt;
      const double freqo1 = M_PI * sig->fdot * dt * dt;
      freqo0 += 2. * freqo1 * N * dseg;
+     e->signal_valid = false;
      if (freqo0 / (2 * M_PI * dt) < sig->fpo || freqo0 / (2 * M_PI * dt) > sig->fpo + sig->B) return TDF_OK;
      SignalParam P;
      P.sinal = std::sin(sig->ra);
@@ -1575,6 +1582,21 @@ int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0_out, 
      e->launches += 2;
      if (h0_out) *h0_out = h0;
      if (in_band) *in_band = 1;
+     e->signal_h0 = h0;
+     e->signal_valid = true;
+     return TDF_OK;
+}
+
+int tdf_engine_get_signal(tdf_engine *e, int32_t det, double *out, int64_t n) {
+     if (!e || !out) return set_error(TDF_ERR_INVALID, "null engine or output");
+     if (det < 0 || det >= e->nifo) return set_error(TDF_ERR_INVALID, "detector %d of %d", det, e->nifo);
+     if (n < e->N) return set_error(TDF_ERR_CAPACITY, "need %d values", e->N);
+     if (!e->signal_valid)
+          return set_error(TDF_ERR_INVALID, "no injected signal held (none added since the last search or upload)");
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaMemcpy(out, e->B0.as<double>() + (size_t)det * e->N, (size_t)e->N * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+     for (int i = 0; i < e->N; i++) out[i] = e->signal_h0 * out[i];   // h0*signadd (init.c:491)
      return TDF_OK;
 }
 

@@ -180,6 +180,23 @@ class Engine:
         _check(self.lib, self.lib.tdf_engine_add_signal(self.h, C.byref(sig), C.byref(h0), C.byref(inb)))
         return h0.value, bool(inb.value)
 
+    def signal(self, det: int, N: int) -> np.ndarray:
+        """h0*s_n[i] (N values) of the signal the last add_signal() injected
+        into detector `det`, before the next search or upload."""
+        out = np.zeros(N, dtype=np.float64)
+        _check(self.lib, self.lib.tdf_engine_get_signal(self.h, int(det), _p(out, C.c_double), N))
+        return out
+
+    def inject(self, job) -> Tuple[float, bool]:
+        """main.c:101-104 for a host.Job: injects job.signal (search:addsig)
+        and, with mods=write_signal, writes the injected signal of every
+        detector as the reference does (init.c:475-497)."""
+        h0, inband = self.add_signal(job.signal)
+        if inband and job.write_signal:
+            from . import host
+            host.write_signal_files(job, [self.signal(n, job.sett.N) for n in range(job.sett.nifo)])
+        return h0, inband
+
     def xdat(self, det: int, n: int) -> np.ndarray:
         """The resident xDat of detector `det` (first n samples)."""
         x = np.zeros(n, dtype=np.float32)

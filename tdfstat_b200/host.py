@@ -529,6 +529,23 @@ def gpu_options(ini: Dict[str, str]) -> GpuOptions:
 # narrow_down_band, read_band_vlines, extract_band_vlines: tdfstat_b200/vlines.py
 
 
+# ---------------------------------------------------------------- injection output
+
+def write_signal_files(job, signals) -> List[str]:
+    """mods=write_signal (init.c:475-497): per detector the injected signal
+    h0*s_n[i], i < N, one "%e" value per line, into
+    <outdir>/injections/signal_<seg>_<band>_<det><label>; returns the paths."""
+    d = os.path.join(job.outdir, "injections")
+    os.makedirs(d, exist_ok=True)
+    paths = []
+    for det, sig in zip(job.dets, signals):
+        p = os.path.join(d, "signal_%03d_%04d_%s%s" % (job.seg, job.band, det.name, job.label))
+        with open(p, "w") as f:
+            f.write("".join("%e\n" % v for v in np.asarray(sig, dtype=np.float64)))
+        paths.append(p)
+    return paths
+
+
 # ---------------------------------------------------------------- the job
 
 def read_signal_file(path: str) -> Dict[str, float]:
@@ -597,6 +614,7 @@ class Job:
         label = ini.get("search:label", "")
         self.label = "_" + label if label else ""
         read_o3 = "read_O3" in self.mods
+        self.write_signal = "write_signal" in self.mods   # init.c:476
         segdir = os.path.join(indir, "%03d" % self.seg)
         names = []
         for d in ("H1", "L1", "V1"):   # detectors_settings, settings.c:136-169

@@ -86,6 +86,7 @@ class Case:
     addsig: Optional[Injection] = None          # written as the reference's signal file, not applied
     noise_seed: Optional[int] = None            # set: noise from its own generator (segments sharing a grid)
     label: str = ""
+    mods_extra: str = ""                        # further search:mods words (e.g. write_signal)
 
     def settings(self) -> host.Settings:
         fpo = host.fpo(self.band, self.overlap, self.dt)
@@ -285,7 +286,7 @@ def write_case(root: str, case: Case) -> str:
         "grid_file = grid.bin",
         "usedet = %s" % "".join(case.dets),
         "addsig = %s" % (os.path.join(root, "in", "signal.txt") if case.addsig else ""),
-        "mods = %s" % ("read_O3" if case.read_o3 else ""),
+        "mods = %s" % " ".join(w for w in ("read_O3" if case.read_o3 else "", case.mods_extra) if w),
         "label = %s" % case.label,
         "veto_flag = %d" % case.veto_flag,
         "checkp_flag = 0",

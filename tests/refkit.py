@@ -214,6 +214,8 @@ def load_oracle():
     lib.orc_splintpad.argtypes = [C.c_void_p, _abi.F64P, C.c_int, C.c_int, C.c_void_p]
     lib.orc_add_signal.restype = C.c_int
     lib.orc_add_signal.argtypes = [C.c_void_p, C.POINTER(_abi.TdfSignal), C.POINTER(C.c_double)]
+    lib.orc_add_signal_out.restype = C.c_int
+    lib.orc_add_signal_out.argtypes = [C.c_void_p, C.POINTER(_abi.TdfSignal), C.POINTER(C.c_double), _abi.F64P]
     return lib
 
 
@@ -233,8 +235,22 @@ class OracleSegment:
                 self.xdat.append(x)
                 self.seg.det[n].xdat = x.ctypes.data_as(C.POINTER(C.c_float))
             h0 = C.c_double(0.0)
-            assert oracle.orc_add_signal(C.byref(self.seg), C.byref(job.signal), C.byref(h0)) == 0
+            self.signal = np.zeros((self.seg.nifo, self.seg.N), dtype=np.float64)
+            assert oracle.orc_add_signal_out(C.byref(self.seg), C.byref(job.signal), C.byref(h0),
+                                             self.signal.ctypes.data_as(C.POINTER(C.c_double))) == 0
             self.h0 = h0.value
+
+
+def reference_signal_files(ini: str):
+    """Runs the reference FP64 build on `ini` (its mods holding write_signal)
+    and returns {file name: text} of what it wrote to out/injections."""
+    run_reference(ini, "f64", threads=1)
+    d = os.path.join(os.path.dirname(os.path.abspath(ini)), "out", "injections")
+    out = {}
+    for fn in sorted(os.listdir(d)):
+        with open(os.path.join(d, fn)) as f:
+            out[fn] = f.read()
+    return out
 
 
 def engine_for(job, form="split", **kw):

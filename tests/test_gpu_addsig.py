@@ -93,3 +93,39 @@ def test_upload_replaces_the_injection(golden):
     eng.upload(job.segment())
     np.testing.assert_array_equal(eng.xdat(0, job.sett.N), np.asarray(job.dets[0].xdat, dtype=np.float32))
     eng.close()
+
+
+def test_write_signal_matches_reference(tmp_path):
+    """mods=write_signal: Engine.inject writes the injected signal as the
+    reference's FP64 build does (init.c:475-497).  CUDA's and libm's sin/cos
+    of ~1e8-rad phases may differ in the last bit, which can move a "%e"
+    value by one unit in its last digit, rarely."""
+    import dataclasses
+    import os
+    from golden.cases import CASES
+    from tdfstat_b200 import host, synth
+    from tdfstat_b200.engine import TdfError
+    case = dataclasses.replace(CASES["g4_addsig"], mods_extra="write_signal")
+    ref = refkit.reference_signal_files(synth.write_case(str(tmp_path / "ref"), case))
+    for form in ("fp64", "split"):
+        job = host.Job(synth.write_case(str(tmp_path / form), case), float_build=(form == "split"))
+        eng = Engine.from_job(job, form=form)
+        h0, inband = eng.inject(job)
+        assert inband and h0 == job.signal.h0
+        d = os.path.join(job.outdir, "injections")
+        assert sorted(os.listdir(d)) == sorted(ref)
+        for fn in ref:
+            with open(os.path.join(d, fn)) as f:
+                mine = f.read().splitlines()
+            theirs = ref[fn].splitlines()
+            assert len(mine) == len(theirs) == job.sett.N
+            diff = [k for k, (a, b) in enumerate(zip(mine, theirs)) if a != b]
+            assert len(diff) <= 2, diff[:5]
+            a = np.array([float(x) for x in mine])
+            b = np.array([float(x) for x in theirs])
+            assert np.all(np.abs(a - b) <= 1e-6 * np.abs(b) + 1e-300)
+        # the engine reuses that memory: no signal is held after a search
+        eng.search(*job.sky_points())
+        with pytest.raises(TdfError):
+            eng.signal(0, job.sett.N)
+        eng.close()

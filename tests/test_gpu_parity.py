@@ -1,7 +1,7 @@
 """GPU parity: libtdfcuda (through its C ABI) against the reference's own
 records (golden fixtures) and the FP64 restatement oracle.
 
-Tolerances (BASELINE north star):
+Tolerances:
   FP64 form  : F relative error <= 1e-10, identical trigger set
   split form : F relative error <= 1e-4, identical trigger set except
                triggers whose F lies within 1e-4 (relative) of thr or of a
@@ -156,4 +156,37 @@ def test_injection_recovered(golden):
     inj = g.case.injections[0]
     assert Fbest > 200
     assert abs(f_hz - inj.f) < 5 * st.B * 2 / st.nfftf * 10
+    eng.close()
+
+
+@pytest.mark.parametrize("form", ["fp64", "split"])
+@pytest.mark.parametrize("variant", ["hemi1", "label", "usedet_H1", "overlap"])
+def test_option_variants_match_reference(tmp_path, variant, form):
+    """The option variants of test_host_options (one hemisphere, a label,
+    usedet selecting one detector, a band overlap) through the GPU engine
+    against the reference's own FP64 run."""
+    import os
+    from tdfstat_b200 import host, synth
+    from test_host_options import _case
+    case, usedet = _case(variant)
+    ini = synth.write_case(str(tmp_path), case)
+    if usedet:
+        with open(ini) as f:
+            text = f.read()
+        with open(ini, "w") as f:
+            f.write(text.replace("usedet = %s" % "".join(case.dets), "usedet = %s" % usedet))
+    if not os.path.exists(refkit.REF_BIN["f64"]):
+        pytest.skip("reference build not present")
+    ref, _, _ = refkit.run_reference(ini, "f64", threads=1)
+    job = host.Job(ini, float_build=(form == "split"))
+    pm, mm, nn = job.sky_points()
+    eng = _engine(job, form)
+    rec = _as_records(eng.search(pm, mm, nn), pm)
+    assert len(rec) == len(ref) > 0
+    np.testing.assert_array_equal(rec.pm, ref.pm)
+    np.testing.assert_array_equal(rec.hdr[:, :3], ref.hdr[:, :3])
+    r = _match(rec, ref, form, case.thr)
+    assert not r["unmatched"], r["unmatched"][:10]
+    assert r["max_F_rel"] <= TOL[form], r["max_F_rel"]
+    assert r["only_a"] + r["only_b"] <= max(2, 0.002 * r["matched"])
     eng.close()

@@ -190,3 +190,31 @@ def test_option_variants_match_reference(tmp_path, variant, form):
     assert r["max_F_rel"] <= TOL[form], r["max_F_rel"]
     assert r["only_a"] + r["only_b"] <= max(2, 0.002 * r["matched"])
     eng.close()
+
+
+@pytest.mark.parametrize("form", ["fp64", "split"])
+def test_candidate_overflow_falls_back_to_full_scan(golden, oracle, form):
+    """At thr = 0.5 about 90% of the bins are candidates (F of noise is
+    chi^2_4 / 2), more than the 64 x 4096 entries of a lane's candidate list
+    for every full group of 64 templates: the row pass stops appending and
+    k_resolve scans every bin instead.  Records against the oracle at the
+    same threshold."""
+    g = golden("g2_h1l1_inj")
+    job = g.job if form == "fp64" else g.job32
+    seg = job.segment()
+    opts = job.search_opts()
+    opts.thr = 0.5
+    pm, mm, nn = job.sky_points()
+    from tdfstat_b200.engine import Engine
+    eng = Engine(seg, opts, form=form)
+    rec = _as_records(eng.search(pm, mm, nn), pm)
+    eng.close()
+    oseg, oopts = g.job.segment(), g.job.search_opts()
+    oopts.thr = 0.5
+    st, ref, _ = refkit.search_points(oracle.orc_search_points, oseg, oopts, pm, mm, nn)
+    assert st == 0 and len(rec) == len(ref) > 64
+    assert ref.ntrig > 100 * len(ref)          # the candidate lists overflowed
+    r = _match(rec, ref, form, 0.5)
+    assert not r["unmatched"], r["unmatched"][:10]
+    assert r["max_F_rel"] <= TOL[form], r["max_F_rel"]
+    assert r["only_a"] + r["only_b"] <= max(2, 0.002 * r["matched"])

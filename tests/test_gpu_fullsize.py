@@ -113,3 +113,28 @@ def test_fullsize_injection_is_loudest(workload, name):
     assert Fbest > 40
     assert abs(f_hz - inj.f) < 50 * bin_hz
     eng.close()
+
+
+def test_trigger_buffer_grows_and_reruns(workload, oracle):
+    """More triggers in one batch than the device trigger buffer holds
+    (2^21 at first): at thr = 0.5 one cfg2 sky point gives ~21k triggers per
+    spindown, 121 spindowns ~2.5M.  The engine grows the buffer and reruns
+    the batch; records against the FP64 oracle at the same threshold."""
+    wl, j64 = workload("cfg2")
+    seg, opts = j64.segment(), j64.search_opts()
+    opts.thr = 0.5
+    ip = wl.centre
+    pm, mm, nn = wl.pm[ip:ip + 1], wl.mm[ip:ip + 1], wl.nn[ip:ip + 1]
+    sst = np.array([opts.spndr[1] - 120], dtype=np.float32)
+    eng = Engine(seg, opts, form="fp64")
+    res = eng.search(pm, mm, nn, sst=sst)
+    eng.close()
+    assert len(res) == 121 and res.ntrig > (1 << 21)
+    rec = refkit.Records(res.hdr, res.pairs, np.repeat(pm, res.per_point))
+    st, ref, _ = refkit.search_points(oracle.orc_search_points, seg, opts, pm, mm, nn, sst=sst,
+                                      max_pairs=res.pairs_flat.size + (1 << 20))
+    assert st == 0 and len(ref) == 121
+    r = refkit.compare_records(rec, ref, f_rtol=1e-12, F_rtol=TOL["fp64"], thr=0.5, tie_band=TOL["fp64"])
+    assert not r["unmatched"], r["unmatched"][:10]
+    assert r["max_F_rel"] <= TOL["fp64"], r["max_F_rel"]
+    assert r["only_a"] + r["only_b"] <= 2

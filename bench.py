@@ -1,15 +1,18 @@
 """Benchmark of the coherent-search hot path (job_core chain) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tdf|reference]
-                    [--form split|fp64] [--workload cfg2|cfg1|cfg3]
+                    [--form split|fp64] [--workload cfg3|cfg2|cfg1|cfg4|cfg5]
+                    [--sweep]
 
-Workload (default cfg2): H1+L1, 2-sidereal-day segment at dt = 2 s
-(N = 86164, nfft = nfftf = 2^17, Ninterp = 2^18), seeded Gaussian noise
-(sigma 1, 5% gaps) plus an injected CW signal (network SNR 12, f = 100.1234 Hz,
-fdot = -3e-10 Hz/s), a 32 x 32 sky patch around the injection x 401
-spindowns = 410,624 templates per step, F over bins [1024, 64512], thr 14.5.
-A step is one pass of the hot path over the whole patch.  Inputs are synthetic
-(no public data set is used).
+Workload (default cfg3, the precision form): H1+L1, 6-sidereal-day segment
+at dt = 2 s (N = 258492, nfft = nfftf = 2^18, Ninterp = 2^19), seeded
+Gaussian noise (sigma 1, 5% gaps) plus four injected CW signals, a 128 x 64
+sky patch around the first injection x 401 spindowns = 3,284,992 templates,
+F over bins [1024, 130048], thr 14.5.  A step searches one 1024-point slice
+of the patch (410,624 templates); consecutive steps take the slices in turn,
+so 8 steps cover the whole patch.  (cfg2: the 2-day segment, N = 86164,
+nfftf = 2^17, a 32 x 32 patch searched whole in every step.)  Inputs are
+synthetic (no public data set is used).
 
   value : templates/s with the segment resident in HBM (device-only pass:
           sky stage + spindown stage + trigger compaction), CUDA events on
@@ -18,13 +21,18 @@ A step is one pass of the hot path over the whole patch.  Inputs are synthetic
   e2e   : the same through the C ABI with host buffers: upload of the
           segment's inputs (xdat, DetSSB, aux arrays) and download of the
           records inside every step.
+  fp64  : the plain FP64 form (the reference's PREC=DOUBLE arithmetic on the
+          GPU) on the same slices, its own warm-up, timing and clock record.
   --impl reference: the reference's own C search (its unmodified sources,
           PREC=FLOAT, built by oracle/Makefile) on the host cores, each step
-          a bounded sample (2 sky points x 401 spindowns) of the workload.
-Under torchrun (N > 1) every rank searches its own 32 x 32 patch (the same
-region, shifted by a fraction of a grid step per rank) as a contiguous shard
-of one point list: weak scaling, no collective on the data path; the
-whole-job value counts all ranks' templates; rank 0 prints the JSON line.
+          a bounded sample (1 sky point x the spindowns) of the workload.
+  --sweep (cfg5): one line per sky-patch size 2^10 .. 2^18 points x 801
+          spindowns; sizes above --sweep-cap points are timed on their first
+          --sweep-cap points (every template counted is searched).
+Under torchrun (N > 1) every rank searches its own patch (the same region,
+shifted by a fraction of a grid step per rank) as a contiguous shard of one
+point list: weak scaling, no collective on the data path; the whole-job
+value counts all ranks' templates; rank 0 prints the JSON line.
 """
 from __future__ import annotations
 
@@ -112,21 +120,6 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(workload: str, form: str):
-    """DRAM bytes per template of the column pass, from the committed ncu
-    summary profiles/traffic_<workload>_<form>.md (its k_colpass table row),
-    or None when there is no summary for this workload and form."""
-    p = os.path.join(REPO, "profiles", "traffic_%s_%s.md" % (workload, form))
-    if not os.path.exists(p):
-        return None
-    with open(p) as f:
-        for line in f:
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if cells and cells[0] == "k_colpass" and len(cells) >= 6:
-                return float(cells[5].split()[0])
-    return None
-
-
 def cpu_reference_sample(wl: Workload, root: str, npts: int, threads: int):
     """Runs the reference FLOAT build on `npts` sky points of the workload
     (directed_range patch of the same segment); returns (templates, seconds,
@@ -154,12 +147,12 @@ def cpu_fft_proxy(nfftf: int, threads: int, ntmpl: int, secs: float):
     2 single-precision transforms of nfftf per template (jobcore.c:477-478)
     timed with the shim as the reference binary has it (oracle/_ref/
     fft-time-f32: same flags, `threads` OpenMP threads, own process, half a
-    second of warm-up, ~1 s timed) and with scipy.fft (pocketfft; one
-    transform does not use several workers, so this is a single-thread
-    time).  The per-sky-point interpolation transforms (FP64, 4 per
-    detector per point) are left in.  When the isolated shim time exceeds
-    the sample's own time the share is reported as measured and no
-    substituted rate is derived."""
+    second of warm-up, ~1 s timed) and with scipy.fft (pocketfft) batched
+    the way a threaded host search would issue them: the 2 transforms of
+    each of `threads` templates in one call with workers = threads.  The
+    per-sky-point interpolation transforms (FP64, 4 per detector per point)
+    are left in.  When the isolated shim time exceeds the sample's own time
+    the share is reported as measured and no substituted rate is derived."""
     import time as _t
     import numpy as _np
     try:
@@ -176,19 +169,23 @@ def cpu_fft_proxy(nfftf: int, threads: int, ntmpl: int, secs: float):
     if r.returncode != 0:
         return None
     t_shim = float(r.stdout.split()[0])
-    x = (_np.random.default_rng(0).standard_normal(nfftf) + 1j * _np.random.default_rng(1).standard_normal(nfftf))
-    x = x.astype(_np.complex64)
+    nb = 2 * max(1, threads)
+    rng = _np.random.default_rng(0)
+    x = (rng.standard_normal((nb, nfftf)) + 1j * rng.standard_normal((nb, nfftf))).astype(_np.complex64)
     t0 = _t.perf_counter()
     while _t.perf_counter() - t0 < 0.3:
-        sfft.fft(x)
+        sfft.fft(x, axis=-1, workers=threads)
+    n = 0
     t0 = _t.perf_counter()
-    for _ in range(100):
-        sfft.fft(x)
-    t_sp = (_t.perf_counter() - t0) / 100
+    while _t.perf_counter() - t0 < 1.0:
+        sfft.fft(x, axis=-1, workers=threads)
+        n += 1
+    t_sp = (_t.perf_counter() - t0) / (n * nb)   # seconds per transform, amortised over the batch
     fft_s = 2 * ntmpl * t_shim
     rest = secs - fft_s
     out = {"fft_share": round(fft_s / secs, 3), "shim_ms_per_fft": round(1e3 * t_shim, 3),
-           "scipy_ms_per_fft_1thread": round(1e3 * t_sp, 3)}
+           "scipy_ms_per_fft": round(1e3 * t_sp, 4),
+           "scipy_batch": "%d transforms per call, workers=%d" % (nb, threads)}
     if rest > 0:
         out["value_with_scipy_fft"] = round(ntmpl / (rest + 2 * ntmpl * t_sp), 2)
     else:
@@ -199,11 +196,45 @@ def cpu_fft_proxy(nfftf: int, threads: int, ntmpl: int, secs: float):
 
 # ------------------------------------------------------------------ arms
 
+def _slices(pm, mm, nn, size):
+    """The point list cut into consecutive slices of `size` points (the last
+    may be shorter); step k searches slice k mod len."""
+    size = len(pm) if size <= 0 else min(size, len(pm))
+    return [(pm[i:i + size], mm[i:i + size], nn[i:i + size]) for i in range(0, len(pm), size)]
+
+
+def _timed_steps(eng, stream, flush, slices, k0, steps, barrier, device):
+    """`steps` device-only steps (slices k0, k0+1, ...) between CUDA events
+    on the engine's stream, the 256 MiB L2 flush before each, clocks
+    sampled during the region.  Returns (ms, templates, triggers, launches,
+    clocks)."""
+    import torch
+    launches0 = eng.launch_count()
+    clocks = ClockSampler(device)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ntrig = nsearched = 0
+    ev0.record(stream)
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()   # 256 MiB (> L2) written between steps, on the engine's stream
+        pm, mm, nn = slices[(k0 + k) % len(slices)]
+        nrec, nt = eng.search_device(pm, mm, nn)
+        ntrig += nt
+        nsearched += nrec
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    return ev0.elapsed_time(ev1), nsearched, ntrig, eng.launch_count() - launches0, clk
+
+
 def run_tdf(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
-    from tdfstat_b200.engine import Engine, load_library
-    import ctypes as C
+    from tdfstat_b200.engine import Engine
 
     torch.cuda.set_device(local_rank)
     root = tempfile.mkdtemp(prefix="tdfbench_")
@@ -215,99 +246,95 @@ def run_tdf(args, rank, world, local_rank):
             pm, mm, nn = pm[:args.sky_points], mm[:args.sky_points], nn[:args.sky_points]
             wl.config["sky_points"] = len(pm)
             wl.config["templates_per_step"] = len(pm) * wl.nspd
+        slice_pts = args.slice_points if args.slice_points is not None else (1024 if args.workload == "cfg3" else 0)
+        slices = _slices(pm, mm, nn, slice_pts)
         seg, opts = job.segment(), job.search_opts()
-        eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
-        lib = load_library()
-        stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
         flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
         def barrier():
             if world > 1:
                 dist.barrier()
 
+        def reduce(vals, op):
+            t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+            if world > 1:
+                dist.all_reduce(t, op=op)
+            return [float(v) for v in t]
+
+        eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
+        stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
         # chunk size by the engine's autotuner on a 16-point sample (untimed)
         tuned = eng.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
         # warm-up steps are the timed step exactly (the flush included: its
         # first launch loads torch's fill kernel)
-        for _ in range(args.warmup):
+        for k in range(args.warmup):
             with torch.cuda.stream(stream):
                 flush.zero_()
-            eng.search_device(pm, mm, nn)
+            eng.search_device(*slices[k % len(slices)])
         torch.cuda.synchronize()
-        # templates a step searches = records it writes (one per spindown of
-        # every point inside the grid ellipse)
-        ntmpl, _ = eng.search_device(pm, mm, nn)
-        if ntmpl != len(pm) * wl.nspd:
-            print("bench: %d of %d patch templates lie inside the sky grid" % (ntmpl, len(pm) * wl.nspd),
-                  file=sys.stderr)
         # ---- value: device-resident inputs, K steps
-        launches0 = eng.launch_count()
-        clocks = ClockSampler(local_rank)
-        clocks.start()
-        barrier()
-        torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ntrig = 0
-        nsearched = 0
-        ev0.record(stream)
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()   # 256 MiB (> L2) written between steps, on the engine's stream
-            nrec, nt = eng.search_device(pm, mm, nn)
-            ntrig += nt
-            nsearched += nrec
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        clk = clocks.stop()
-        ms = ev0.elapsed_time(ev1)
-        launches = eng.launch_count() - launches0
-        # ---- per-kernel durations: the same K steps again with CUDA events
-        # recorded on the engine's stream around every launch.  Timing runs
-        # the kernels one after another (one lane); each launch gets at
-        # least 32 templates (1024 column-pass CTAs, 3.5 waves at 2 per SM)
-        # so that a launch has the GPU to itself rather than under-filling it
+        ms, nsearched, ntrig, launches, clk = _timed_steps(eng, stream, flush, slices, 0, args.steps, barrier,
+                                                           local_rank)
+        if nsearched != sum(len(slices[k % len(slices)][0]) for k in range(args.steps)) * wl.nspd:
+            print("bench: some patch points lie outside the sky grid", file=sys.stderr)
+        # ---- per-kernel durations: one or two steps again at the run's own
+        # chunk size, CUDA events recorded on the engine's stream around every
+        # launch (kernels one after another: one lane)
         tc_run = eng.templates_per_chunk
-        tc_timed = max(tc_run, 32)
-        eng.templates_per_chunk = tc_timed
         eng.enable_kernel_timing(True)
-        for _ in range(args.steps):
+        for k in range(max(1, min(args.steps, 2))):
             with torch.cuda.stream(stream):
                 flush.zero_()
-            eng.search_device(pm, mm, nn)
+            eng.search_device(*slices[k % len(slices)])
         torch.cuda.synchronize()
         ktimes = eng.kernel_times()
         eng.enable_kernel_timing(False)
-        eng.templates_per_chunk = tc_run
         # ---- e2e: host buffers through the C ABI
-        for _ in range(1):
-            eng.upload(seg)
-            eng.search(pm, mm, nn)
+        eng.upload(seg)
+        eng.search(*slices[0])
         torch.cuda.synchronize()
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         nsearched_e2e = 0
-        for _ in range(args.steps):
+        d2h = 0
+        for k in range(args.steps):
             eng.upload(seg)
-            res = eng.search(pm, mm, nn)
+            res = eng.search(*slices[k % len(slices)])
             nsearched_e2e += len(res)
+            d2h += len(res) * 40 + res.pairs_flat.nbytes
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
         ms_e2e = e0.elapsed_time(e1)
         h2d = sum(d.xdat.nbytes + d.detssb.nbytes for d in job.dets) + job.cosmodf.nbytes + job.sinmodf.nbytes \
-            + pm.nbytes + mm.nbytes + nn.nbytes
-        d2h = len(res) * 40 + res.pairs_flat.nbytes
+            + sum(a.nbytes for a in slices[0])
+        eng.close()
+        # ---- the plain FP64 form on the same slices (its own engine)
+        fp64 = None
+        if args.form == "split" and not args.no_fp64:
+            e64 = Engine(seg, opts, form="fp64", device=local_rank, max_sky_batch=args.sky_batch)
+            s64 = torch.cuda.ExternalStream(e64.stream(), device=local_rank)
+            # 48 templates per chunk: the autotuner's choice for this form at every size measured
+            # (timing the candidates in FP64 would take minutes)
+            e64.templates_per_chunk = t64 = 48
+            k64 = max(1, min(args.steps, args.fp64_steps))
+            for k in range(max(1, min(args.warmup, 2))):
+                with torch.cuda.stream(s64):
+                    flush.zero_()
+                e64.search_device(*slices[k % len(slices)])
+            torch.cuda.synchronize()
+            ms64, n64, _, _, clk64 = _timed_steps(e64, s64, flush, slices, 0, k64, barrier, local_rank)
+            e64.close()
+            ms64, = reduce([ms64], dist.ReduceOp.MAX)
+            n64, = reduce([n64], dist.ReduceOp.SUM)
+            fp64 = {"value": round(n64 / (ms64 / 1e3), 1), "unit": UNIT, "steps": k64,
+                    "ms_per_step": round(ms64 / k64, 3), "templates_per_chunk": t64, "clocks": clk64}
         # times: max over ranks; templates searched: sum over ranks
-        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-        n = torch.tensor([nsearched, nsearched_e2e], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        ms, ms_e2e = float(t[0]), float(t[1])
-        value = float(n[0]) / (ms / 1e3)
-        e2e = float(n[1]) / (ms_e2e / 1e3)
+        ms, ms_e2e = reduce([ms, ms_e2e], dist.ReduceOp.MAX)
+        nsum, nsum_e2e = reduce([nsearched, nsearched_e2e], dist.ReduceOp.SUM)
+        value = nsum / (ms / 1e3)
+        e2e = nsum_e2e / (ms_e2e / 1e3)
         out = None
         if rank == 0:
             peak, peak_kind = measured_peaks()
@@ -320,46 +347,104 @@ def run_tdf(args, rank, world, local_rank):
                 per_launch_bytes = bt * col_t / col_n
                 avg_s = col_ms / col_n / 1e3
                 achieved = per_launch_bytes / avg_s / 1e9
-                tr = profile_traffic(args.workload, args.form)
-                traffic = round(tr * col_t / col_n) if tr is not None else None
                 roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                        "frac": round(achieved / peak, 4), "traffic": traffic,
+                        "frac": round(achieved / peak, 4), "traffic": None,
                         "kernel": "k_colpass (demodulation + first FFT pass)",
                         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                         "algorithmic_bytes_per_template": bt,
-                        "kernel_ms_share": {k: round(v, 3) for k, v in ktimes.items() if k.endswith("_ms")},
+                        "kernel_ms": {k: round(v, 3) for k, v in ktimes.items() if k.endswith("_ms")},
                         "avg_launch_ms": round(col_ms / col_n, 4), "templates_per_launch": col_t / col_n,
-                        "timed": "CUDA events on the engine stream around each launch, one lane, %d templates "
-                                 "per launch (the run itself: %d per chunk over concurrent lanes)" % (tc_timed, tc_run)}
+                        "timed": "CUDA events on the engine stream around each launch, one lane, the run's "
+                                 "%d templates per launch" % tc_run,
+                        "traffic_note": "DRAM bytes are not counted in this run (no profiler in the timed "
+                                        "process); ncu figures of the same kernel are kept under profiles/"}
             cpu = None
             if not args.no_cpu_baseline and world == 1:   # the CPU baseline is an N = 1 figure
-                r = cpu_reference_sample(wl, tempfile.mkdtemp(prefix="tdfcpu_"), 3, os.cpu_count() or 1)
+                r = cpu_reference_sample(wl, tempfile.mkdtemp(prefix="tdfcpu_"), 1, os.cpu_count() or 1)
                 if r:
                     nrec_c, secs = r
                     cpu = {"value": round(nrec_c / secs, 2), "unit": UNIT, "cores": os.cpu_count(),
                            "kind": "reference",
                            "fft": cpu_fft_proxy(job.sett.nfftf, os.cpu_count() or 1, nrec_c, secs),
-                           "sample": "%d templates (3 sky points x %d spindowns) of the same workload, reference "
+                           "sample": "%d templates (1 sky point x %d spindowns) of the same workload, reference "
                                      "search sources PREC=FLOAT built with the project FFTW-API shim "
                                      "(textbook radix-2 FFT; FFTW absent), %.1f s" % (nrec_c, wl.nspd, secs)}
+            per_step = int(round(nsum / args.steps))
             out = {
                 "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
-                "data": "synthetic (seeded Gaussian noise + injected CW signal, synthetic ephemeris)",
+                "data": "synthetic (seeded Gaussian noise + injected CW signals, synthetic ephemeris)",
                 "config": dict(wl.config, form=args.form, templates_per_chunk=tuned,
-                               templates_searched_per_step_per_gpu=int(ntmpl),
-                               templates_searched_per_step=int(round(float(n[0]) / args.steps)),
+                               step=("one %d-point slice of the %d-point patch per step, slices in turn"
+                                     % (len(slices[0][0]), len(pm)) if len(slices) > 1
+                                     else "the whole patch per step"),
+                               templates_searched_per_step=per_step,
                                l2="flush: 256 MiB write between timed steps; per-step working set > L2"),
                 "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                        "d2h_bytes_per_step": int(d2h)},
+                        "d2h_bytes_per_step": int(d2h // args.steps)},
                 "gpu_launches": int(launches),
                 "triggers_per_step": int(ntrig // args.steps),
+                "fp64": fp64,
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             }
-        eng.close()
         return out
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
+def run_sweep(args, rank, world, local_rank):
+    """cfg5 scale sweep on one GPU: sky patches of 2^10 .. 2^18 points x 801
+    spindowns of the same segment (N = 258492, sigma 1.0 / 1.3, 10% gaps).
+    Each size is one device-only search over the patch's first
+    min(size, --sweep-cap) points, timed with CUDA events after one untimed
+    warm-up search of 64 points; every template counted is searched.  Prints
+    one JSON line per size."""
+    import torch
+    from tdfstat_b200.engine import Engine
+
+    if world > 1 or rank != 0:
+        return None
+    torch.cuda.set_device(local_rank)
+    root = tempfile.mkdtemp(prefix="tdfsweep_")
+    try:
+        wl = Workload("cfg5", root)
+        job = wl.job
+        seg, opts = job.segment(), job.search_opts()
+        eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
+        stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        tuned = eng.autotune(wl.pm[:16], wl.mm[:16], wl.nn[:16]) if not args.no_autotune else None
+        peak, peak_kind = measured_peaks()
+        bt = len(job.dets) * job.sett.N * (24 if args.form == "split" else 40)
+        for k in range(10, 19):
+            npts = 1 << k
+            pm, mm, nn = wl.patch(npts)
+            timed = min(npts, args.sweep_cap)
+            sl = [(pm[:timed], mm[:timed], nn[:timed])]
+            eng.search_device(pm[:64], mm[:64], nn[:64])
+            torch.cuda.synchronize()
+            ms, nsearched, ntrig, launches, clk = _timed_steps(eng, stream, flush, sl, 0, 1, lambda: None,
+                                                               local_rank)
+            value = nsearched / (ms / 1e3)
+            ach = value * bt / 1e9
+            print(json.dumps({
+                "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+                "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
+                "data": "synthetic (seeded Gaussian noise, sigma 1.0 / 1.3, 10% gaps, injected CW signal)",
+                "config": dict(wl.config, sky_points=npts, templates_per_step=npts * wl.nspd,
+                               timed_sky_points=timed, templates_searched=int(nsearched),
+                               form=args.form, templates_per_chunk=tuned,
+                               patch="%d x %d points over 3.2 x 3.2 grid cells" % (1 << (k // 2), 1 << (k - k // 2)),
+                               timed=("the whole patch" if timed == npts else
+                                      "the patch's first %d points (every template counted is searched)" % timed)),
+                "hbm": {"achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+                        "algorithmic_bytes_per_template": bt, "peak_kind": peak_kind},
+                "gpu_launches": int(launches), "triggers": int(ntrig), "clocks": clk}), flush=True)
+        eng.close()
+        return None
     finally:
         shutil.rmtree(root, ignore_errors=True)
 
@@ -504,10 +589,13 @@ def run_reference(args, rank, world):
         sample = ("%d templates per step (1 sky point x %d spindowns) of the %s workload; reference search "
                   "sources (PREC=FLOAT, SIMD=NONE) compiled unmodified against the project FFTW-API shim "
                   "(textbook radix-2 FFT, FFTW absent)" % (tot_n // args.steps, wl.nspd, wl.name))
+        config = dict(wl.config, sky_points=1, templates_per_step=tot_n // args.steps,
+                      step="one sky point of the workload's segment x its spindowns (a bounded sample of the "
+                           "GPU arm's workload; same segment, grid, F range and threshold)")
         return {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * tot_s / args.steps, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic", "config": dict(wl.config),
+                "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "cores": threads, "kind": "reference",
                                  "sample": sample, "fft": fftp},
                 "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -522,13 +610,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tdf", choices=["tdf", "reference"])
     ap.add_argument("--form", default="split", choices=["split", "fp64"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
+    ap.add_argument("--workload", default="cfg3", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
+    ap.add_argument("--slice-points", type=int, default=None,
+                    help="sky points per step (default: 1024 for cfg3, the whole patch otherwise)")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form's line entry")
+    ap.add_argument("--fp64-steps", type=int, default=3, help="timed steps of the FP64 form (at most --steps)")
     ap.add_argument("--sky-batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--segments-by-cost", action="store_true",
                     help="cfg4 on several GPUs: whole segments to ranks by estimated cost (strong scaling)")
     ap.add_argument("--sky-points", type=int, default=0, help="use only the first K sky points (profiling runs)")
+    ap.add_argument("--sweep", action="store_true", help="cfg5: one line per sky-patch size 2^10 .. 2^18")
+    ap.add_argument("--sweep-cap", type=int, default=4096, help="sky points timed per sweep size at most")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -541,6 +635,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         out = run_reference(args, rank, world)
+    elif args.sweep:
+        if args.workload != "cfg5":
+            ap.error("--sweep is the cfg5 scale sweep (--workload cfg5)")
+        out = run_sweep(args, rank, world, local_rank)
     elif args.workload == "cfg4":
         out = run_tdf_segments(args, rank, world, local_rank)
     else:

@@ -276,15 +276,20 @@ int tdf_coincidences(const tdf_coinc_opts *opts, int32_t nseg, const tdf_coinc_s
    het1, spnd: the template's phase coefficients (FP64); aa, bb: the network
    sums of the amplitude modulation (jobcore.c:373-386).  The intermediate
    spectra and FFT tables live in one static device array of the library
-   (about 4.2 MB, held on every GPU that loads the library until the
+   (about 4.3 MB, held on every GPU that loads the library until the
    process exits), so nfftf is limited to 2^18 (4096 <= nfftf <= 2^18,
    power of two, N <= nfftf, 1 <= nifo <= 8); larger sizes are rejected with
-   TDF_ERR_UNSUPPORTED.  The first call on a device resolves the array's
-   device address (and any call with a new nfftf rebuilds the tables in it);
-   make that first call before capturing a stream.  All calls share the one
-   array: calls whose work overlaps on the GPU (other streams, other host
-   threads) race, so serialise them.  Work is enqueued on `stream`
-   (cudaStream_t, NULL = default stream) and completes asynchronously. */
+   TDF_ERR_UNSUPPORTED.  The array holds the FFT tables of every supported
+   nfftf.  The first call on a device (and the first after the device's
+   context was reset) resolves the array's device address, writes all the
+   tables on `stream` and waits for them there (a one-time synchronisation);
+   it is refused with TDF_ERR_INVALID while `stream` is being captured, so
+   make it outside any capture.  Later calls only read the tables.  All
+   calls share the one array's spectra and parameters, which keep the last
+   call's contents: calls whose work overlaps on the GPU (other streams,
+   other host threads) race, so serialise them.  Work is enqueued on
+   `stream` (cudaStream_t, NULL = default stream) and completes
+   asynchronously. */
 int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, int32_t nifo, int32_t N, int32_t Nal,
                               int32_t nfftf, double het1, double spnd, float aa, float bb,
                               int32_t fr0, int32_t fr1, float *d_F, void *stream);

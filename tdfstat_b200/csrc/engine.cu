@@ -1775,24 +1775,64 @@ int tdf_engine_get_kernel_times(tdf_engine *e, tdf_kernel_times *out) {
 // the FFT twiddle tables and the template parameters -- is the static array
 // below, so a call allocates nothing.  Host code must not pass the array's
 // name to a kernel (on the host it is only a stand-in); the device address is
-// resolved once per device with cudaGetSymbolAddress.
+// resolved with cudaGetSymbolAddress, once per device context.
+//
+// The array holds one set of twiddle tables for every supported transform
+// length (2^12 .. 2^18), all written once when a device context is first
+// seen, so no later call rewrites state that earlier enqueued work (or a
+// replayed graph) reads.
 
 namespace {
 
+constexpr int kStaticMinLog2 = 12;
 constexpr int kStaticMaxLog2 = 18;                                  // nfftf <= 2^18
 constexpr size_t kStaticY = 2ull * (1ull << kStaticMaxLog2) * sizeof(float2);   // two spectra
-constexpr size_t kStaticTab = (512 + 512 + 256 + 1024) * sizeof(float2);         // line1, line2, hi, lo
+
+// float2 entries of the tables of a 2^l transform: line tables of N1 and N2
+// points, four-step hi (2^l / 1024) and lo (1024)
+constexpr int static_n1(int l) { return 1 << ((l + 1) / 2); }
+constexpr int static_n2(int l) { return 1 << (l / 2); }
+constexpr int static_nhi(int l) { return l >= 10 ? 1 << (l - 10) : 1; }
+constexpr size_t static_tab_entries(int l) { return (size_t)static_n1(l) + static_n2(l) + static_nhi(l) + 1024; }
+constexpr size_t static_tab_offset(int l) {   // float2 entries before the tables of 2^l
+     return l <= kStaticMinLog2 ? 0 : static_tab_offset(l - 1) + static_tab_entries(l - 1);
+}
+constexpr size_t kStaticTab = static_tab_offset(kStaticMaxLog2 + 1) * sizeof(float2);
 constexpr size_t kStaticPar = 256;                                  // TmplParam + AaBb
 constexpr size_t kStaticBytes = kStaticY + kStaticTab + kStaticPar;
+static_assert(kStaticTab % 16 == 0, "parameter block alignment");
 
 struct StaticDevState {
-     bool ready = false;
-     unsigned char *base = nullptr;   // device address of g_static_scratch on this device
-     int tables_for = 0;              // nfftf the tables currently hold
+     unsigned long long ctx = 0;      // id of the device context the state below belongs to (0: none yet)
+     unsigned char *base = nullptr;   // device address of g_static_scratch in that context
 };
 constexpr int kStaticMaxDevices = 64;
 StaticDevState g_static_dev[kStaticMaxDevices];
 std::mutex g_static_mu;
+
+// id of the calling thread's current CUDA context (cuCtxGetId, through the
+// runtime's driver entry points); 0 when it cannot be read
+unsigned long long current_context_id() {
+     static std::once_flag once;
+     static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+     static PFN_cuCtxGetId_v12000 get_id = nullptr;
+     std::call_once(once, [] {
+          void *p = nullptr;
+          cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+          if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+              q == cudaDriverEntryPointSuccess)
+               get_cur = (PFN_cuCtxGetCurrent_v4000)p;
+          p = nullptr;
+          if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+              q == cudaDriverEntryPointSuccess)
+               get_id = (PFN_cuCtxGetId_v12000)p;
+     });
+     if (!get_cur || !get_id) return 0;
+     CUcontext c = nullptr;
+     unsigned long long id = 0;
+     if (get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+     return id;
+}
 
 }  // namespace
 
@@ -1824,7 +1864,7 @@ extern "C" int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, i
 {
      if (!d_xab || !d_s2 || !d_F) return set_error(TDF_ERR_INVALID, "null device pointer");
      if (nifo < 1 || nifo > TDF_MAX_DETECTORS) return set_error(TDF_ERR_INVALID, "nifo=%d", nifo);
-     if (!pow2(nfftf) || nfftf < 4096)
+     if (!pow2(nfftf) || nfftf < (1 << kStaticMinLog2))
           return set_error(TDF_ERR_INVALID, "nfftf=%d must be a power of two >= 4096", nfftf);
      if (nfftf > (1 << kStaticMaxLog2))
           return set_error(TDF_ERR_UNSUPPORTED, "nfftf=%d exceeds the static scratch limit 2^%d of tdf_fstat_operands_static",
@@ -1837,28 +1877,42 @@ extern "C" int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, i
      if (dev < 0 || dev >= kStaticMaxDevices) return set_error(TDF_ERR_UNSUPPORTED, "device %d", dev);
      cudaStream_t st = (cudaStream_t)stream;
      const int l = ilog2i(nfftf);
-     const int N1 = 1 << ((l + 1) / 2), N2 = nfftf / N1;
+     const int N1 = static_n1(l), N2 = static_n2(l);
      unsigned char *base;
      {
           std::lock_guard<std::mutex> lk(g_static_mu);
           StaticDevState &S = g_static_dev[dev];
-          if (!S.ready) {
-               void *p = nullptr;
-               CUCHK(cudaGetSymbolAddress(&p, g_static_scratch));
+          // the symbol's address in the current context (this also makes
+          // the runtime set the context up), then that context's id: a new
+          // context (first call, or after cudaDeviceReset) gets its array's
+          // tables written before anything reads them
+          void *p = nullptr;
+          CUCHK(cudaGetSymbolAddress(&p, g_static_scratch));
+          const unsigned long long ctx = current_context_id();
+          if (!ctx || ctx != S.ctx || (unsigned char *)p != S.base) {
+               cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+               CUCHK(cudaStreamIsCapturing(st, &cs));
+               if (cs != cudaStreamCaptureStatusNone)
+                    return set_error(TDF_ERR_INVALID, "tdf_fstat_operands_static: the first call on a device (which "
+                                     "writes the FFT tables) must not be made while its stream is being captured");
+               float2 *tabs = (float2 *)((unsigned char *)p + kStaticY);
+               for (int k = kStaticMinLog2; k <= kStaticMaxLog2; k++) {
+                    float2 *t = tabs + static_tab_offset(k);
+                    const int n1 = static_n1(k), n2 = static_n2(k);
+                    k_static_tables<<<(1024 + 255) / 256, 256, 0, st>>>(t, n1, t + n1, n2, t + n1 + n2,
+                                                                         t + n1 + n2 + static_nhi(k), 1 << k);
+                    CUCHK(cudaGetLastError());
+               }
+               // later calls may come on other streams: the tables are complete first
+               CUCHK(cudaStreamSynchronize(st));
                S.base = (unsigned char *)p;
-               S.ready = true;
+               S.ctx = ctx;
           }
           base = S.base;
-          float2 *tab = (float2 *)(base + kStaticY);
-          if (S.tables_for != nfftf) {
-               k_static_tables<<<(1024 + 255) / 256, 256, 0, st>>>(tab, N1, tab + 512, N2, tab + 1024, tab + 1280, nfftf);
-               CUCHK(cudaGetLastError());
-               S.tables_for = nfftf;
-          }
      }
      float2 *Y = (float2 *)base;
-     float2 *tab = (float2 *)(base + kStaticY);
-     const float2 *line1 = tab, *line2 = tab + 512, *hi = tab + 1024, *lo = tab + 1280;
+     const float2 *tab = (const float2 *)(base + kStaticY) + static_tab_offset(l);
+     const float2 *line1 = tab, *line2 = tab + N1, *hi = tab + N1 + N2, *lo = tab + N1 + N2 + static_nhi(l);
      TmplParam *tp = (TmplParam *)(base + kStaticY + kStaticTab);
      AaBb *ab = (AaBb *)(base + kStaticY + kStaticTab + 128);
      TmplParam t;

@@ -7,7 +7,9 @@
         -3e-10 Hz/s), a 32 x 32 sky patch around the injection (step 0.25
         grid cells) x 401 spindowns = 410,624 templates
   cfg3  as cfg2 with N = 258492 (6 days), nfft = 2^18, Ninterp = 2^19,
-        a 128 x 64 patch (step 0.1 cells) x 401 spindowns = 3,284,992 templates
+        four injections (network SNR 20, 8, 12, 16 at 100.12, 100.05, 100.18,
+        100.22 Hz), a 128 x 64 patch (step 0.1 cells) around the first x 401
+        spindowns = 3,284,992 templates
   cfg4  64 segments, nod cycling through 2, 3, 4, 6 (N = 86164, 129246,
         172328, 258492; nfft 2^17, 2^17, 2^18, 2^18), per-segment seeds, noise
         and gaps, H1+L1; a 16 x 16 patch x 401 spindowns per segment =
@@ -45,9 +47,14 @@ def workload_case(name: str):
     # sky grid's ellipse: every patch point is searched (job_core skips
     # points outside it, jobcore.c:248)
     if name == "cfg3":
-        inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
+        # four signals at network SNR 20, 8, 12, 16; the patch is centred on
+        # the first, the others lie elsewhere in the sky and the band
+        injs = (synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=20.0),
+                synth.Injection(f=100.0517, fdot=-1e-10, ra=1.1, dec=-0.4, iota=0.3, psi=1.2, phase=0.7, snr=8.0),
+                synth.Injection(f=100.1788, fdot=-6e-10, ra=2.6, dec=0.2, iota=1.4, psi=0.1, phase=4.1, snr=12.0),
+                synth.Injection(f=100.2231, fdot=-2e-10, ra=5.3, dec=-1.1, iota=2.0, psi=0.8, phase=5.5, snr=16.0))
         return synth.Case(dt=2.0, nod=6, band=360, dets=("H1", "L1"), seed=303, thr=14.5, fdot_step=1e-10,
-                          sky_cells=16.0, injections=(inj,)), (128, 64), 401, 0.1
+                          sky_cells=16.0, injections=injs), (128, 64), 401, 0.1
     inj = synth.Injection(f=100.1234, fdot=-3e-10, ra=4.0, dec=0.9, iota=0.9, psi=0.4, phase=2.2, snr=12.0)
     return synth.Case(dt=2.0, nod=2, band=360, dets=("H1", "L1"), seed=202, thr=14.5, fdot_step=1e-10,
                       sky_cells=16.0, injections=(inj,)), (32, 32), 401, 0.25
@@ -91,6 +98,7 @@ class Workload:
             mms.append((m0 + mg.ravel()).astype(np.float32))
             nns.append((n0 + ng.ravel()).astype(np.float32))
         self.pm, self.mm, self.nn = np.concatenate(pms), np.concatenate(mms), np.concatenate(nns)
+        self.m0, self.n0, self.pm0 = m0, n0, pm0[0]
         self.nspd = nspd
         self.shape = (nm, nn_)
         self.centre = (nm // 2) * nn_ + nn_ // 2   # index of the patch centre (the injection's grid point)
@@ -99,6 +107,19 @@ class Workload:
                        "nfftf": job.sett.nfftf, "Ninterp": job.sett.Ninterp, "sky_points": nm * nn_,
                        "spindowns": nspd, "templates_per_step": self.templates,
                        "fr": list(job.range.fr), "thr": c.thr}
+
+    def patch(self, npts: int, extent: float = 3.2):
+        """A square-ish patch of npts = 2^k sky points around the same centre,
+        spanning `extent` grid cells in mm and nn (the spacing shrinks as
+        the patch grows, so that every point stays inside the grid's
+        ellipse).  Returns (pm, mm, nn)."""
+        k = int(round(np.log2(npts)))
+        assert 1 << k == npts
+        a, b = 1 << (k // 2), 1 << (k - k // 2)
+        step = extent / max(a, b)
+        mg, ng = np.meshgrid((np.arange(a) - a // 2) * step, (np.arange(b) - b // 2) * step, indexing="ij")
+        pm = np.full(npts, self.pm0, dtype=np.int32)
+        return pm, (self.m0 + mg.ravel()).astype(np.float32), (self.n0 + ng.ravel()).astype(np.float32)
 
     def shard(self, rank: int, world: int):
         return shard_points(self.pm, self.mm, self.nn, rank, world)

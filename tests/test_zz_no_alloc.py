@@ -7,9 +7,11 @@ static device array of the library, so it takes only caller-owned buffers.
 The test builds the spindown operands of a sky point on the CPU (the FP64
 oracle's sky stage), places them in device memory the test itself allocates
 (the caller's buffers), calls the entry point through the C ABI for two
-templates in a row and checks each F spectrum against the engine entry
-point tdf_fstat_spectrum() for the same template, at the split form's
-tolerance (1e-4, normalised per bin by max(F, 1)).  This file is collected
+templates in a row, then at another transform length, detector count and
+row stride, and checks each F spectrum against the engine entry point
+tdf_fstat_spectrum() for the same template and against the FP64 oracle's
+orc_fstat_spectrum(), at the split form's tolerance (1e-4, normalised per
+bin by max(F, 1)).  This file is collected
 last so that a failure here stops a -x run only after every other test ran.
 """
 import ctypes as C
@@ -71,44 +73,75 @@ def _split_sums(oracle, job, pm, mm, nn):
     return float(tot_a), float(tot_b)
 
 
-def test_static_scratch_entry_matches_engine(golden, oracle):
+def _call_case(lib, oracle, golden, name, nk, pad):
+    """nk calls in a row for consecutive spindowns of the first sky point of
+    golden case `name`, operands in caller buffers of row stride N + pad;
+    each F spectrum checked against the engine's tdf_fstat_spectrum and the
+    FP64 oracle's orc_fstat_spectrum."""
     import torch
     from tdfstat_b200 import _abi
-    from tdfstat_b200.engine import Engine, load_library
+    from tdfstat_b200.engine import Engine
 
-    lib = load_library()
-    g = golden("g2_h1l1_inj")
+    g = golden(name)
     job = g.job32
     pm, mm, nn = job.sky_points()
     p, m, n = int(pm[0]), float(mm[0]), float(nn[0])
     xab, s2 = _operands(oracle, job, p, m, n)
     aa, bb = _split_sums(oracle, job, p, m, n)
     N, nifo, nfftf = job.sett.N, job.sett.nifo, job.sett.nfftf
+    Nal = N + pad
+    if pad:
+        xp = np.zeros((nifo, Nal, 4), np.float32)
+        sp = np.zeros((nifo, Nal), np.float32)
+        xp[:, :N] = xab.reshape(nifo, N, 4)
+        sp[:, :N] = s2.reshape(nifo, N)
+        xab, s2 = xp.reshape(-1, 4), sp.reshape(-1)
     fr0, fr1 = job.range.fr
     dev = torch.device("cuda", 0)
     d_xab = torch.from_numpy(xab).to(dev).contiguous()     # the caller's buffers
     d_s2 = torch.from_numpy(s2).to(dev).contiguous()
     d_F = torch.zeros(fr1 - fr0 + 1, dtype=torch.float32, device=dev)
     eng = Engine.from_job(job, form="split")
+    seg64, opts64 = g.job.segment(), g.job.search_opts()
     M = job.sett.M
     ss0 = float(job.range.spndr[0])
-    for k in range(2):                 # two calls in a row share the static scratch
+    for k in range(nk):
         ss = float(np.float32(ss0 + k * job.range.sstep))
         spnd = ss * M[5] + n * M[9] + m * M[13]
         het1 = math.fmod(ss * M[4], M[0])
         if het1 < 0:
             het1 += M[0]
-        d_F.zero_()
-        st = lib.tdf_fstat_operands_static(d_xab.data_ptr(), d_s2.data_ptr(), nifo, N, N, nfftf, het1, spnd,
+        d_F.fill_(-1.0)
+        st = lib.tdf_fstat_operands_static(d_xab.data_ptr(), d_s2.data_ptr(), nifo, N, Nal, nfftf, het1, spnd,
                                            aa, bb, fr0, fr1, d_F.data_ptr(), None)
         assert st == _abi.TDF_OK, lib.tdf_last_error()
         torch.cuda.synchronize()
         F_static = d_F.double().cpu().numpy()
         F_engine = eng.fstat(p, m, n, ss)
-        err = np.max(np.abs(F_static - F_engine) / np.maximum(F_engine, 1.0))
-        print("call", k, "max normalised F difference", err)
-        assert err <= TOL, err
+        F_oracle = np.zeros_like(F_engine)
+        assert oracle.orc_fstat_spectrum(C.byref(seg64), C.byref(opts64), p, m, n, ss,
+                                         F_oracle.ctypes.data_as(C.POINTER(C.c_double)), len(F_oracle)) == 0
+        e_eng = np.max(np.abs(F_static - F_engine) / np.maximum(F_engine, 1.0))
+        e_orc = np.max(np.abs(F_static - F_oracle) / np.maximum(F_oracle, 1.0))
+        print(name, "nfftf", nfftf, "Nal-N", pad, "call", k, "max normalised F difference: engine %.3g, "
+              "oracle %.3g" % (e_eng, e_orc))
+        assert e_eng <= TOL, e_eng
+        assert e_orc <= TOL, e_orc
     eng.close()
+
+
+def test_static_scratch_entry_matches_engine(golden, oracle):
+    """Two calls in a row at one transform length (nfftf 2^14, two
+    detectors), then a second length (nfftf 2^13, one detector) with
+    operand rows padded beyond N, a three-detector network, and the first
+    length again: the tables of every length stay valid side by side."""
+    from tdfstat_b200.engine import load_library
+
+    lib = load_library()
+    _call_case(lib, oracle, golden, "g2_h1l1_inj", 2, 0)
+    _call_case(lib, oracle, golden, "g1_h1_directed", 1, 1000)
+    _call_case(lib, oracle, golden, "g6_h1l1v1", 1, 0)
+    _call_case(lib, oracle, golden, "g2_h1l1_inj", 1, 0)
 
 
 def test_static_scratch_entry_rejects_oversize():

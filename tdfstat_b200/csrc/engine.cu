@@ -195,7 +195,7 @@ struct DevBuf {
 template <typename T>
 struct FFTTables {
      int N = 0, N1 = 0, N2 = 0;
-     DevBuf line1, line2, hi, lo;
+     DevBuf line1, line2, hi, lo, base, step;
      int build(int n) {
           N = n;
           int l = ilog2i(n);
@@ -215,6 +215,20 @@ struct FFTTables {
           CUCHK(cudaMemcpy(lo.p, o.data(), 1024 * sizeof(cx<T>), cudaMemcpyHostToDevice));
           return TDF_OK;
      }
+     // per-thread base twiddles of the column-pass epilogue (StoreFourstepG):
+     // base[t*N2 + n2] = W^(n2*t), t < N1/8, and step[n2] = W^(n2*N1/8)
+     int build_base() {
+          const int R = N1 / 8;
+          std::vector<cx<T>> b((size_t)R * N2), st(N2);
+          for (int t = 0; t < R; t++)
+               for (int n2 = 0; n2 < N2; n2++) b[(size_t)t * N2 + n2] = tw((long)n2 * t, N);
+          for (int n2 = 0; n2 < N2; n2++) st[n2] = tw((long)n2 * R, N);
+          TRY(base.alloc(b.size() * sizeof(cx<T>)));
+          TRY(step.alloc(st.size() * sizeof(cx<T>)));
+          CUCHK(cudaMemcpy(base.p, b.data(), b.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+          CUCHK(cudaMemcpy(step.p, st.data(), st.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+          return TDF_OK;
+     }
      static cx<T> tw(long m, long n) {
           // e^{-2 pi i m/n}; m/n exact for power-of-two n
           double a = -2.0 * M_PI * ((double)(m % n) / (double)n);
@@ -230,7 +244,7 @@ struct FFTTables {
           CUCHK(cudaMemcpy(b.p, v.data(), L * sizeof(cx<T>), cudaMemcpyHostToDevice));
           return TDF_OK;
      }
-     void release() { line1.release(); line2.release(); hi.release(); lo.release(); }
+     void release() { line1.release(); line2.release(); hi.release(); lo.release(); base.release(); step.release(); }
      const cx<T> *l1() const { return line1.as<cx<T>>(); }
      const cx<T> *l2() const { return line2.as<cx<T>>(); }
      const cx<T> *h() const { return hi.as<cx<T>>(); }
@@ -304,7 +318,8 @@ struct tdf_engine {
           DevBuf Fbuf;    // F ring of a resolve group
           DevBuf mubuf;   // blocks_avg means of a resolve group
           DevBuf tcnt;    // per-template trigger counts + candidate count
-          DevBuf cand;    // candidate bins of a resolve group
+          DevBuf cand;    // candidate bins of a resolve group (uint2), or the sparse store's records (uint4)
+          DevBuf Ebuf;    // sparse F store: edge ring of a resolve group (split form)
      };
      static constexpr int kMaxLanes = 4;
      Lane ln[kMaxLanes];
@@ -333,10 +348,12 @@ struct tdf_engine {
      // captured launches bake in; captured on the second sighting of a key
      struct GraphKey {
           int slot, nt, Tc, Gt, lanes;
+          bool sparse;
           const void *tp, *trig;
           unsigned long long trig_cap;
           bool operator==(const GraphKey &o) const {
-               return slot == o.slot && nt == o.nt && Tc == o.Tc && Gt == o.Gt && lanes == o.lanes && tp == o.tp &&
+               return slot == o.slot && nt == o.nt && Tc == o.Tc && Gt == o.Gt && lanes == o.lanes &&
+                      sparse == o.sparse && tp == o.tp &&
                       trig == o.trig && trig_cap == o.trig_cap;
           }
      };
@@ -352,6 +369,12 @@ struct tdf_engine {
      uint64_t graph_tick = 0;
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
      bool row_bulk = true;     // row passes fetch their rows by bulk copies (TDF_ROW_BULK=0: per thread)
+     // split form: the row pass keeps F on the chip and hands over only the
+     // candidates and the edge bins of its runs (TDF_FULL_F=1: full F ring);
+     // blocks_avg, and a batch that needs more of the spectrum, use the full
+     // store.  sparse_now is the store the current search uses.
+     bool sparse_f = true;
+     bool sparse_now = false;
      // optional per-kernel event timing
      bool timing = false;
      tdf_kernel_times kt{};
@@ -598,7 +621,9 @@ static int engine_alloc(tdf_engine *e) {
           TRY(L.mubuf.alloc(G * std::max(1, e->nblk_mu) * rsz));
           TRY(L.tcnt.alloc((G + 1) * sizeof(unsigned)));
           CUCHK(cudaMemset(L.tcnt.p, 0, L.tcnt.bytes));
-          TRY(L.cand.alloc(e->cand_cap * sizeof(uint2)));
+          TRY(L.cand.alloc(e->cand_cap * sizeof(uint4)));
+          // edge ring: 2 floats per (template, row CTA, k2) = nfftf bytes per template
+          if (e->form == TDF_FORM_SPLIT) TRY(L.Ebuf.alloc(G * (size_t)e->nfftf));
      }
      TRY(e->linesd.alloc(std::max<size_t>(1, e->lines.size()) * sizeof(double)));
      if (!e->lines.empty())
@@ -614,7 +639,10 @@ static int engine_alloc(tdf_engine *e) {
      CUCHK(cudaMallocHost((void **)&e->h_cnt, 4 * sizeof(unsigned long long)));
      TRY(e->t_nfft.build(e->nfft));
      TRY(e->t_ninterp.build(e->Ninterp));
-     if (e->form == TDF_FORM_SPLIT) TRY(e->t_f32.build(e->nfftf));
+     if (e->form == TDF_FORM_SPLIT) {
+          TRY(e->t_f32.build(e->nfftf));
+          TRY(e->t_f32.build_base());
+     }
      else TRY(e->t_f64.build(e->nfftf));
      TRY(staged_setup(e));
      return TDF_OK;
@@ -640,6 +668,7 @@ static void engine_free(tdf_engine *e) {
           L.mubuf.release();
           L.tcnt.release();
           L.cand.release();
+          L.Ebuf.release();
      }
      e->t_nfft.release();
      e->t_ninterp.release();
@@ -834,6 +863,56 @@ static cudaStream_t lane_stream(const tdf_engine *e, int l) { return l == 0 ? e-
 // at most Gt templates (one chunk when a chunk is larger)
 static int group_templates(const tdf_engine *e) { return std::max(1, e->Gt / e->Tc) * e->Tc; }
 
+// Split-form spindown passes with the four-step geometry fixed at compile
+// time for the transform lengths of the benchmark sizes (nfftf 2^15 .. 2^18,
+// two detectors); every other case takes the same policies with the
+// geometry read at run time.
+template <int L, int N2C>
+static int launch_split_col_c(dim3 grid, const DemodSplitIL &p, const StoreFourstepG<0> &g, const float2 *tw,
+                              cudaStream_t st) {
+     DemodSplitILT<N2C, 2> pro{p.xab, p.s2, p.tp, p.N, p.N2, p.Nal, p.nifo};
+     StoreFourstepG<N2C> epi{g.y, g.w0, g.ws, g.N2, g.N};
+     return launch_col_L<float, L, -1, 2>(grid, pro, epi, tw, st);
+}
+
+static int launch_split_col(int nifo, int N1, int N2, dim3 grid, const DemodSplitIL &pro, const StoreFourstepG<0> &epi,
+                            const float2 *tw, cudaStream_t st) {
+     if (nifo == 2) {
+          if (N1 == 512 && N2 == 512) return launch_split_col_c<512, 512>(grid, pro, epi, tw, st);
+          if (N1 == 512 && N2 == 256) return launch_split_col_c<512, 256>(grid, pro, epi, tw, st);
+          if (N1 == 256 && N2 == 256) return launch_split_col_c<256, 256>(grid, pro, epi, tw, st);
+          if (N1 == 256 && N2 == 128) return launch_split_col_c<256, 128>(grid, pro, epi, tw, st);
+     }
+     return launch_col<float, -1, 2>(N1, grid, pro, epi, tw, st);
+}
+
+template <int L, int N1C, bool HALF>
+static int launch_split_row_c(dim3 grid, const RowsYBulk<float> &src, const StoreFstatT<0, false> &f,
+                              const float2 *tw, cudaStream_t st) {
+     StoreFstatT<N1C, HALF> epi{f.F, f.tp, f.ab, f.nF, f.fr0, f.fr1, f.N1, f.thr, f.cand, f.cand_cnt, f.cand_cap, f.boff,
+                                f.E, f.scand};
+     return launch_row_L<float, L, -1, 2>(grid, src, epi, tw, st);
+}
+
+template <int L, int N1C>
+static int launch_split_row_h(bool half, dim3 grid, const RowsYBulk<float> &src, const StoreFstatT<0, false> &f,
+                              const float2 *tw, cudaStream_t st) {
+     return half ? launch_split_row_c<L, N1C, true>(grid, src, f, tw, st)
+                 : launch_split_row_c<L, N1C, false>(grid, src, f, tw, st);
+}
+
+// the row pass keeps only bins <= fr1; with fr1 < nfftf/2 = N1*N2/2 every
+// kept output has k2 < N2/2
+static int launch_split_row(int N1, int N2, int fr1, dim3 grid, const RowsYBulk<float> &src,
+                            const StoreFstatT<0, false> &epi, const float2 *tw, cudaStream_t st) {
+     const bool half = (int64_t)fr1 < (int64_t)N1 * N2 / 2;
+     if (N2 == 512 && N1 == 512) return launch_split_row_h<512, 512>(half, grid, src, epi, tw, st);
+     if (N2 == 256 && N1 == 512) return launch_split_row_h<256, 512>(half, grid, src, epi, tw, st);
+     if (N2 == 256 && N1 == 256) return launch_split_row_h<256, 256>(half, grid, src, epi, tw, st);
+     if (N2 == 128 && N1 == 256) return launch_split_row_h<128, 256>(half, grid, src, epi, tw, st);
+     return launch_row<float, -1, 2>(N2, grid, src, epi, tw, st);
+}
+
 template <typename T>
 static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt) {
      cudaStream_t st = lane_stream(e, l);
@@ -846,9 +925,10 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
      const TmplParam *ctp = dtp + boff;
      const unsigned G = (unsigned)group_templates(e);
      unsigned *tcnt = Ln.tcnt.as<unsigned>();
-     StoreFourstep<T, -1, 2> epi{Ln.Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
      size_t tev = e->timing ? timing_begin(e, st) : (size_t)-1;
      if constexpr (std::is_same<T, float>::value) {
+          StoreFourstepG<0> epi{Ln.Ybuf.as<float2>(), t.base.template as<float2>(), t.step.template as<float2>(), t.N2,
+                                e->nfftf};
           if (e->staged) {
                DemodSplitStaged pro;
                pro.mx = e->tm_x[e->cur];
@@ -866,26 +946,45 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
           } else {
                DemodSplitIL pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal,
                                 e->nifo};
-               TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
+               TRY(launch_split_col(e->nifo, t.N1, t.N2, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st));
           }
      } else {
+          StoreFourstep<T, -1, 2> epi{Ln.Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
           DemodFP64 pro{e->xa64[e->cur].as<double2>(), e->xb64[e->cur].as<double2>(), e->t1[e->cur].as<double>(), ctp,
                         e->N, t.N2, e->Nal, e->nifo};
           TRY((launch_col<T, -1, 2>(t.N1, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st)));
      }
      if (e->timing) timing_end(e, tev, KT_COL, nt, st);
      const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
-     StoreFstat<T> epi2{Ln.Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF, e->opts.fr[0],
-                        e->opts.fr[1], t.N1, e->opts.thr, blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G,
-                        e->cand_cap, boff};
      tev = e->timing ? timing_begin(e, st) : (size_t)-1;
-     if (e->row_bulk) {
-          RowsYBulk<T> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2,
-                           reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1)};
-          TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+     unsigned *errw = reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1);
+     if constexpr (std::is_same<T, float>::value) {
+          StoreFstatT<0, false> epi2{Ln.Fbuf.as<float>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF,
+                                     e->opts.fr[0], e->opts.fr[1], t.N1, e->opts.thr,
+                                     blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, boff};
+          if (e->sparse_now) {
+               epi2.cand = nullptr;
+               epi2.E = Ln.Ebuf.as<float>();
+               epi2.scand = Ln.cand.as<uint4>();
+          }
+          if (e->row_bulk) {
+               RowsYBulk<float> src{Ln.Ybuf.as<float2>(), e->nfftf, t.N2, errw};
+               TRY(launch_split_row(t.N1, t.N2, e->opts.fr[1], dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st));
+          } else {
+               RowsY<float, 2> src{Ln.Ybuf.as<float2>(), e->nfftf, t.N2};
+               TRY((launch_row<float, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+          }
      } else {
-          RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
-          TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+          StoreFstat<T> epi2{Ln.Fbuf.as<T>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(), e->nF,
+                             e->opts.fr[0], e->opts.fr[1], t.N1, e->opts.thr,
+                             blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, boff};
+          if (e->row_bulk) {
+               RowsYBulk<T> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2, errw};
+               TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+          } else {
+               RowsY<T, 2> src{Ln.Ybuf.as<cx<T>>(), e->nfftf, t.N2};
+               TRY((launch_row<T, -1, 2>(t.N2, dim3(t.N1 / LINES, nt), src, epi2, t.l2(), st)));
+          }
      }
      if (e->timing) timing_end(e, tev, KT_ROW, nt, st);
      e->launches += 2;
@@ -928,6 +1027,10 @@ static int run_resolve(tdf_engine *e, int l, const TmplParam *dtp, int ntg) {
           if (split) k_threshold<T, false><<<g, 256, 0, st>>>(Ln.Fbuf.as<T>(), Ln.mubuf.as<T>(), A);
           else k_threshold<T, true><<<g, 256, 0, st>>>(Ln.Fbuf.as<T>(), Ln.mubuf.as<T>(), A);
           e->launches += 2;
+     } else if (split && e->sparse_now) {
+          SparseArgs S{Ln.Ebuf.as<float>(), Ln.cand.as<uint4>(), tcnt + G, e->cand_cap, e->t_f32.N1, e->t_f32.N2};
+          k_resolve_sparse<<<64, 256, 0, st>>>(A, S);
+          e->launches++;
      } else {
           if (split) k_resolve<T, false><<<64, 256, 0, st>>>(Ln.Fbuf.as<T>(), A, Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
           else k_resolve<T, true><<<64, 256, 0, st>>>(Ln.Fbuf.as<T>(), A, Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, ntg);
@@ -979,7 +1082,8 @@ static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
 static int run_templates_batch(tdf_engine *e, int nt) {
      const TmplParam *dtp = e->tparam.as<TmplParam>();
      if (!e->use_graphs || e->timing) return run_templates(e, dtp, nt);
-     const tdf_engine::GraphKey k{e->cur, nt, e->Tc, e->Gt, e->nlanes, e->tparam.p, e->trig[e->cur].p, e->trig_cap};
+     const tdf_engine::GraphKey k{e->cur, nt, e->Tc, e->Gt, e->nlanes, e->sparse_now, e->tparam.p, e->trig[e->cur].p,
+                                  e->trig_cap};
      size_t gi = e->graphs.size();
      for (size_t i = 0; i < e->graphs.size(); i++)
           if (e->graphs[i].key == k) gi = i;
@@ -1046,7 +1150,7 @@ static int ensure_tparam(tdf_engine *e, size_t n) {
 
 // Waits for the batch last run in `slot`, checks its flags and collects its
 // triggers; *over is set when the trigger buffer was too small.
-static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_total, bool *over) {
+static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_total, bool *over, bool *need_full) {
      CUCHK(cudaEventSynchronize(e->done[slot]));
      if (e->timing) timing_collect(e);
      const unsigned long long nfound = e->h_cnt[2 * slot];
@@ -1055,6 +1159,10 @@ static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_tot
           return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
      if (errf & ERR_STAGE_TIMEOUT)
           return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
+     if (errf & ERR_NEED_FULL_F) {
+          *need_full = true;
+          return TDF_OK;
+     }
      if (nfound > e->trig_cap) {
           *over = true;
           e->h_cnt[2 * slot] = nfound;   // keep the needed size visible
@@ -1103,7 +1211,8 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
           maxnt = std::max(maxnt, nt);
      }
      TRY(ensure_tparam(e, maxnt));
-     for (int attempt = 0;; attempt++) {
+     e->sparse_now = e->sparse_f && e->form == TDF_FORM_SPLIT && !(e->opts.blocks_avg && e->nblk_mu > 0);
+     for (int grown = 0;;) {
           e->h_trig.clear();
           *ntrig_total = 0;
           CUCHK(cudaStreamSynchronize(e->sky_stream));
@@ -1111,16 +1220,16 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
           for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
           for (int l = 0; l < e->nlanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
           int pending[2] = {0, 0};
-          bool over = false;
+          bool over = false, need_full = false;
           size_t b = 0;
           for (size_t b0 = 0; b0 < inside.size(); b0 += e->Bs, b++) {
                const int slot = (int)(b & 1);
                // the slot's previous batch must be drained before its staging
                // and trigger buffer are reused; the other slot keeps running
                if (pending[slot]) {
-                    TRY(finish_slot(e, slot, collect, ntrig_total, &over));
+                    TRY(finish_slot(e, slot, collect, ntrig_total, &over, &need_full));
                     pending[slot] = 0;
-                    if (over) break;
+                    if (over || need_full) break;
                }
                e->cur = slot;
                const int nb = (int)std::min<size_t>(e->Bs, inside.size() - b0);
@@ -1160,16 +1269,23 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
                pending[slot] = 1;
           }
           // drain in batch order: the slot of the second-to-last batch first
-          for (int k = 0; k < 2 && !over; k++) {
+          for (int k = 0; k < 2 && !over && !need_full; k++) {
                const int slot = (int)((b + k) & 1);
                if (pending[slot]) {
-                    TRY(finish_slot(e, slot, collect, ntrig_total, &over));
+                    TRY(finish_slot(e, slot, collect, ntrig_total, &over, &need_full));
                     pending[slot] = 0;
                }
           }
           CUCHK(cudaStreamSynchronize(e->stream));
+          if (need_full) {
+               // a MAX_ALG 3 tie or more candidates than the list holds: the
+               // whole search again with the full F store
+               if (!e->sparse_now) return set_error(TDF_ERR_CUDA, "trigger selection asked for the full F store twice");
+               e->sparse_now = false;
+               continue;
+          }
           if (!over) break;
-          if (attempt > 2) return set_error(TDF_ERR_CAPACITY, "trigger buffer could not be sized");
+          if (++grown > 3) return set_error(TDF_ERR_CAPACITY, "trigger buffer could not be sized");
           // a batch found more triggers than the buffer holds: grow and rerun
           unsigned long long need = std::max(e->h_cnt[0], e->h_cnt[2]);
           e->trig_cap = std::max<unsigned long long>(need + (need >> 2), e->trig_cap * 2);
@@ -1347,6 +1463,8 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
      const char *gr = getenv("TDF_GRAPHS");
      if (gr && gr[0] == '0') e->use_graphs = false;
+     const char *ff = getenv("TDF_FULL_F");
+     if (ff && ff[0] == '1') e->sparse_f = false;
      const char *rb = getenv("TDF_ROW_BULK");
      if (rb && rb[0] == '0') e->row_bulk = false;
      const char *gt = getenv("TDF_GROUP_TEMPLATES");
@@ -1636,6 +1754,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[0], sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
      CUCHK(cudaMemsetAsync(e->counters[0].p, 0, 2 * sizeof(unsigned long long), e->stream));
      for (int l = 0; l < e->nlanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+     e->sparse_now = false;   // the spectrum itself is the output: the full F store
      TRY(run_templates(e, e->tparam.as<TmplParam>(), 1));
      CUCHK(cudaMemcpyAsync(e->h_cnt, e->counters[0].p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
      CUCHK(cudaStreamSynchronize(e->stream));

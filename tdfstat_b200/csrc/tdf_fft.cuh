@@ -164,24 +164,43 @@ __device__ __forceinline__ void pass_dft(V (&v)[8]) {
      }
 }
 
+// Output r of butterfly j of a pass of span NS goes to line position
+// base + r*NS, base = (j/NS)*NS*R + j%NS, stored at pad8(position).  The
+// padded addresses are formed from one per-thread offset: with NS = 1 and
+// R = 8 the outputs are 8j .. 8j+7, i.e. pad8 = 9j + r; with NS a multiple
+// of 8, pad8(base + r*NS) = pad8(base) + r*9*NS/8.  (NS is a constant once
+// line_fft's pass loop is unrolled.)
 template <typename T, int L, int R>
 __device__ __forceinline__ void pass_store(const cx<T> (&v)[8], cx<T> *s, int t, int NS) {
 #pragma unroll
      for (int q = 0; q < 8 / R; q++) {
-          int j = t + q * (L / 8);
-          int base = (j / NS) * NS * R + (j % NS);
+          const int j = t + q * (L / 8);
+          if (NS == 1 && R == 8) {
+               cx<T> *d = s + 9 * j;
 #pragma unroll
-          for (int r = 0; r < R; r++) s[pad8(base + r * NS)] = v[q + r * (8 / R)];
+               for (int r = 0; r < R; r++) d[r] = v[q + r * (8 / R)];
+          } else if (NS % 8 == 0) {
+               cx<T> *d = s + pad8((j / NS) * NS * R + (j % NS));
+#pragma unroll
+               for (int r = 0; r < R; r++) d[r * (NS + NS / 8)] = v[q + r * (8 / R)];
+          } else {
+               const int base = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+               for (int r = 0; r < R; r++) s[pad8(base + r * NS)] = v[q + r * (8 / R)];
+          }
      }
 }
 
+// Input r of butterfly j of the next pass is line position j + r*L/R; L/R is
+// a multiple of 8, so pad8(j + r*L/R) = pad8(j) + r*9*(L/R)/8.
 template <typename T, int L, int R>
 __device__ __forceinline__ void pass_load(cx<T> (&v)[8], const cx<T> *s, int t) {
+     static_assert((L / R) % 8 == 0, "line length per radix must be a multiple of 8");
 #pragma unroll
      for (int q = 0; q < 8 / R; q++) {
-          int j = t + q * (L / 8);
+          const cx<T> *d = s + pad8(t + q * (L / 8));
 #pragma unroll
-          for (int r = 0; r < R; r++) v[q + r * (8 / R)] = s[pad8(j + r * (L / R))];
+          for (int r = 0; r < R; r++) v[q + r * (8 / R)] = d[r * ((L / R) + (L / R) / 8)];
      }
 }
 

@@ -475,7 +475,11 @@ struct DemodSplit {
 // operands are two adjacent 16-byte words and one 8-byte word, each read
 // from one address, and one pointer per operand array steps through the
 // thread's samples.  Same arithmetic, in the same order, as DemodSplit.
-struct DemodSplitIL {
+// CN2 / CNIFO > 0 fix the row length N2 and the detector count at compile
+// time (the thread's eight samples are then constant offsets from one
+// pointer); 0 reads them from the struct.
+template <int CN2 = 0, int CNIFO = 0>
+struct DemodSplitILT {
      const float4 *xab;
      const float *s2;
      const TmplParam *tp;
@@ -483,12 +487,14 @@ struct DemodSplitIL {
 
      template <int L>
      __device__ __forceinline__ void load(float2 (&v)[2][8], int b, int n2, int t) const {
+          const int n2s = CN2 > 0 ? CN2 : N2;
+          const int nf = CNIFO > 0 ? CNIFO : nifo;
           const TmplParam P = tp[b];
           const float spf = (float)P.spnd;
-          const int i0 = N2 * t + n2;
-          const int di = N2 * (L / 8);    // samples between the thread's elements
-          const int de = di * nifo;       // operand words between them
-          const size_t e0 = ((size_t)P.slot * Nal + i0) * nifo;
+          const int i0 = n2s * t + n2;
+          const int di = n2s * (L / 8);   // samples between the thread's elements
+          const int de = di * nf;         // operand words between them
+          const size_t e0 = ((size_t)P.slot * Nal + i0) * nf;
           const float4 *xp = xab + e0;
           const float *sp = s2 + e0;
 #pragma unroll
@@ -502,18 +508,18 @@ struct DemodSplitIL {
                     const float pr = (float)fma(-kk, TWO_PI, ph);
                     const float4 *x = xp + m * de;
                     const float *s = sp + m * de;
-                    if (nifo == 2) {
+                    if (nf == 2) {
                          const float2 ss = __ldg(reinterpret_cast<const float2 *>(s));
                          DemodSplit::rot(__ldg(x), fmaf(spf, ss.x, pr), fa, fb);
                          float2 pa, pb;
                          DemodSplit::rot(__ldg(x + 1), fmaf(spf, ss.y, pr), pa, pb);
                          fa = cadd(fa, pa);
                          fb = cadd(fb, pb);
-                    } else if (nifo == 1) {
+                    } else if (nf == 1) {
                          DemodSplit::rot(__ldg(x), fmaf(spf, __ldg(s), pr), fa, fb);
                     } else {
                          CompSum ar, ai, br, bi;
-                         for (int d = 0; d < nifo; d++) {
+                         for (int d = 0; d < nf; d++) {
                               float2 pa, pb;
                               DemodSplit::rot(__ldg(x + d), fmaf(spf, __ldg(s + d), pr), pa, pb);
                               if (d == 0) { ar.init(pa.x); ai.init(pa.y); br.init(pb.x); bi.init(pb.y); }
@@ -528,6 +534,7 @@ struct DemodSplitIL {
           }
      }
 };
+using DemodSplitIL = DemodSplitILT<0, 0>;
 
 // DemodSplitIL with its operands brought in by TMA.  Thread (c, t) of the CTA
 // needs, for element m, the samples of row n1 = t + m*R (R = L/8) of column
@@ -715,6 +722,111 @@ struct StoreFstat {
      }
 };
 
+// Candidate records of the sparse F store (16 bytes): template (within the
+// resolve group) | kind << 24, bin, F[bin], and one neighbour's F.
+constexpr unsigned CAND_LOCAL = 0u;   // a local maximum decided in the row pass; no tie with bin-1
+constexpr unsigned CAND_LEFT = 1u;    // first bin of a CTA's run of 8: F[bin-1] is in the edge ring (nb = F[bin+1])
+constexpr unsigned CAND_RIGHT = 2u;   // last bin of a run: F[bin+1] is in the edge ring (nb = F[bin-1])
+constexpr unsigned CAND_TIE = 3u;     // F[bin-1] == F[bin]: the MAX_ALG 3 run needs F[bin-2]
+constexpr unsigned ERR_NEED_FULL_F = 4u;   // a batch needs the full F spectra (tie or candidate overflow)
+
+// StoreFstat for the split form with the four-step column count N1 fixed at
+// compile time (CN1 > 0, else the struct's N1) and, when HALF, only the
+// outputs k2 < L/2 of each row formed: every bin the search keeps lies below
+// nfftf/2 (fr1 < N1*L/2), so the upper half of the row transform's last
+// pass is never computed (its outputs are dead).  F = |Fa|^2 * (1/aa) +
+// |Fb|^2 * (1/bb), the reciprocals formed once per thread.
+//
+// Two ways to hand F to the trigger selection:
+//   full (E == nullptr): the whole spectrum [fr0, fr1] goes to the F ring
+//     and the bins passing the threshold test to the candidate list (uint2
+//     {template, bin}); used with blocks_avg and as the fallback.
+//   sparse (E != nullptr): no spectrum leaves the SM.  The 8 lanes c of a
+//     thread group hold the consecutive bins k1b + c + N1*k2 of one k2, so a
+//     bin's neighbours are one shuffle away except at the run's ends: the
+//     row pass decides the local-maximum test itself for c = 1..6 and
+//     writes candidate records (uint4, kinds above) for bins passing the
+//     threshold; only the end bins c = 0 and 7 of every run go to the edge
+//     ring E[((b*NJ + j)*L + k2)*2 + (c == 7)] (j = CTA index) for the
+//     neighbours of the other CTAs' end-bin candidates.
+template <int CN1, bool HALF>
+struct StoreFstatT {
+     float *F;
+     const TmplParam *tp;
+     const AaBb *ab;
+     int nF, fr0, fr1, N1;
+     double thr;
+     uint2 *cand;
+     unsigned *cand_cnt;
+     unsigned cand_cap;
+     int boff;        // index of this chunk's first template within its resolve group
+     float *E = nullptr;       // sparse form: edge ring of the resolve group
+     uint4 *scand = nullptr;   // sparse form: candidate records
+     template <int L>
+     __device__ __forceinline__ void store(const float2 (&v)[2][8], int b, int k1, int t) const {
+          const AaBb s = ab[tp[b].slot];
+          const float ia = 1.f / s.aaf, ib = 1.f / s.bbf;
+          const float thrf = (float)thr;
+          const bool exact_thr = (double)thrf == thr;   // then f < thr compares the same in float
+          const int n1 = CN1 > 0 ? CN1 : N1;
+          if (E == nullptr) {
+               float *dst = F + (size_t)b * nF - fr0;
+#pragma unroll
+               for (int m = 0; m < (HALF ? 4 : 8); m++) {
+                    const int k = k1 + n1 * (t + m * (L / 8));
+                    if (k >= fr0 && k <= fr1) {
+                         const float f = fmaf(cnorm(v[0][m]), ia, cnorm(v[1][m]) * ib);
+                         dst[k] = f;
+                         const bool pass = exact_thr ? !(f < thrf) : !((double)f < thr);
+                         if (cand && pass && k >= fr0 + 1 && k < fr1 - 1) {
+                              const unsigned c = atomicAdd(cand_cnt, 1u);
+                              if (c < cand_cap) cand[c] = make_uint2((unsigned)(b + boff), (unsigned)k);
+                         }
+                    }
+               }
+               return;
+          }
+          const int c = k1 & (LINES - 1);
+          const int nj = n1 / LINES;
+          const unsigned bg = (unsigned)(b + boff);
+          float *ej = E + ((size_t)bg * nj + (k1 >> 3)) * (2 * L) + (c == LINES - 1 ? 1 : 0);
+#pragma unroll
+          for (int m = 0; m < (HALF ? 4 : 8); m++) {
+               const int k2 = t + m * (L / 8);
+               const int k = k1 + n1 * k2;
+               const float f = fmaf(cnorm(v[0][m]), ia, cnorm(v[1][m]) * ib);
+               // neighbours within the run of 8 (lanes c-1, c+1 of the same k2)
+               const float fm = __shfl_up_sync(0xffffffffu, f, 1, LINES);
+               const float fp = __shfl_down_sync(0xffffffffu, f, 1, LINES);
+               if (k >= fr0 && k <= fr1) {
+                    if (c == 0 || c == LINES - 1) ej[2 * k2] = f;
+                    const bool pass = exact_thr ? !(f < thrf) : !((double)f < thr);
+                    if (pass && k >= fr0 + 1 && k < fr1 - 1) {
+                         unsigned kind;
+                         float nb = 0.f;
+                         bool keep = true;
+                         if (c == 0) {
+                              kind = CAND_LEFT;
+                              nb = fp;
+                         } else if (c == LINES - 1) {
+                              kind = CAND_RIGHT;
+                              nb = fm;
+                         } else {
+                              keep = !(fm > f || f < fp);   // a local maximum
+                              kind = fm == f ? CAND_TIE : CAND_LOCAL;
+                         }
+                         if (keep) {
+                              const unsigned q = atomicAdd(cand_cnt, 1u);
+                              if (q < cand_cap)
+                                   scand[q] = make_uint4(bg | (kind << 24), (unsigned)k, __float_as_uint(f),
+                                                         __float_as_uint(nb));
+                         }
+                    }
+               }
+          }
+     }
+};
+
 // blocks_avg means (auxi.c:349-355): mu_j = sum of the j-th block of NAV
 // values of F[fr0..] / (2 NAV).  grid (nblk, ntmpl), 256 threads
 template <typename T>
@@ -766,24 +878,13 @@ struct ThrArgs {
      unsigned *err;
 };
 
-// MAX_ALG 3 (jobcore.c:556-603) as the single-threaded loop executes it:
-// bin i (fr0 < i < fr1-1) is a trigger when it is a local maximum >= thr
-// and the previous accepted bin is not i-1 (the loop's "i++" skip), i.e.
-// when the run of consecutive local-maximum bins ending at i-1 has even
-// length.  Then the veto intervals are checked and the trigger appended.
-template <typename T, bool FP64>
-__device__ __forceinline__ void threshold_bin(const T *__restrict__ F, const T *__restrict__ mu, const ThrArgs &A,
-                                              int b, int i)
+// Appends the trigger at bin i of template b (group-relative) with F value
+// Fc: its frequency (jobcore.c:571) in the emulated build's arithmetic, the
+// veto intervals (jobcore.c:575-583), the per-template count against
+// bufsize/2 (jobcore.c:586-590), then the compacted trigger list.
+template <bool FP64>
+__device__ __forceinline__ void emit_trigger(const ThrArgs &A, int b, int i, double Fc)
 {
-     const int fr0 = A.fr0, nblk = A.nblk;
-     const double thr = A.thr;
-     const T *Fb = F + (size_t)b * A.nF - fr0;
-     const T *mub = mu ? mu + (size_t)b * nblk : nullptr;
-     if (!is_peak(Fb, mub, i, fr0, nblk, thr)) return;
-     int run = 0;
-     for (int k = i - 1; k >= fr0 + 1 && is_peak(Fb, mub, k, fr0, nblk, thr); k--) run++;
-     if (run & 1) return;
-     const T Fc = fval(Fb, mub, i, fr0, nblk);
      const TmplParam P = A.tp[b];
      double fcmp;
      float ff;
@@ -817,6 +918,26 @@ __device__ __forceinline__ void threshold_bin(const T *__restrict__ F, const T *
      }
 }
 
+// MAX_ALG 3 (jobcore.c:556-603) as the single-threaded loop executes it:
+// bin i (fr0 < i < fr1-1) is a trigger when it is a local maximum >= thr
+// and the previous accepted bin is not i-1 (the loop's "i++" skip), i.e.
+// when the run of consecutive local-maximum bins ending at i-1 has even
+// length.  Then the veto intervals are checked and the trigger appended.
+template <typename T, bool FP64>
+__device__ __forceinline__ void threshold_bin(const T *__restrict__ F, const T *__restrict__ mu, const ThrArgs &A,
+                                              int b, int i)
+{
+     const int fr0 = A.fr0, nblk = A.nblk;
+     const double thr = A.thr;
+     const T *Fb = F + (size_t)b * A.nF - fr0;
+     const T *mub = mu ? mu + (size_t)b * nblk : nullptr;
+     if (!is_peak(Fb, mub, i, fr0, nblk, thr)) return;
+     int run = 0;
+     for (int k = i - 1; k >= fr0 + 1 && is_peak(Fb, mub, k, fr0, nblk, thr); k--) run++;
+     if (run & 1) return;
+     emit_trigger<FP64>(A, b, i, (double)fval(Fb, mub, i, fr0, nblk));
+}
+
 // The candidates the row pass collected; when the list overflowed, every
 // bin of the chunk (grid-stride).  grid (G), 256 threads
 template <typename T, bool FP64>
@@ -835,6 +956,62 @@ __global__ void __launch_bounds__(256) k_resolve(const T *__restrict__ F, ThrArg
           const unsigned nb = (unsigned)(A.fr1 - A.fr0 - 2 > 0 ? A.fr1 - A.fr0 - 2 : 0);   // bins fr0+1 .. fr1-2
           for (unsigned long long x = g0; x < (unsigned long long)nt * nb; x += gs)
                threshold_bin<T, FP64>(F, nullptr, A, (int)(x / nb), A.fr0 + 1 + (int)(x % nb));
+     }
+}
+
+// Trigger selection from the sparse F store's candidate records: the
+// missing neighbour of a run's end bin from the edge ring, the local-maximum
+// test, and the trigger append.  A record whose MAX_ALG 3 run needs more of
+// the spectrum (a tie with the previous bin), or a candidate list that
+// overflowed, sets ERR_NEED_FULL_F: the host then reruns the batch with the
+// full F store.  grid (G), 256 threads
+struct SparseArgs {
+     const float *E;
+     const uint4 *cand;
+     const unsigned *cand_cnt;
+     unsigned cand_cap;
+     int N1, L;       // four-step column count and row length
+};
+
+__global__ void __launch_bounds__(256) k_resolve_sparse(ThrArgs A, SparseArgs S)
+{
+     const unsigned n = *S.cand_cnt;
+     if (n > S.cand_cap) {
+          if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(A.err, ERR_NEED_FULL_F);
+          return;
+     }
+     const unsigned gs = gridDim.x * blockDim.x;
+     const int nj = S.N1 / LINES;
+     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gs) {
+          const uint4 r = S.cand[i];
+          const int b = (int)(r.x & 0xffffffu);
+          const unsigned kind = r.x >> 24;
+          const int k = (int)r.y;
+          const float f = __uint_as_float(r.z);
+          if (kind == CAND_TIE) {
+               atomicOr(A.err, ERR_NEED_FULL_F);
+               continue;
+          }
+          if (kind != CAND_LOCAL) {
+               const int k1 = k % S.N1, k2 = k / S.N1, j = k1 / LINES;
+               const float *Eb = S.E + (size_t)b * nj * (2 * S.L);
+               float fm, fp;
+               if (kind == CAND_LEFT) {
+                    // bin k-1: the last bin of the previous CTA's run (or of the last CTA's at k2-1)
+                    fm = j > 0 ? Eb[((size_t)(j - 1) * S.L + k2) * 2 + 1] : Eb[((size_t)(nj - 1) * S.L + (k2 - 1)) * 2 + 1];
+                    fp = __uint_as_float(r.w);
+               } else {
+                    // bin k+1: the first bin of the next CTA's run (or of the first CTA's at k2+1)
+                    fp = j < nj - 1 ? Eb[((size_t)(j + 1) * S.L + k2) * 2] : Eb[((size_t)k2 + 1) * 2];
+                    fm = __uint_as_float(r.w);
+               }
+               if (fm > f || f < fp) continue;   // not a local maximum
+               if (fm == f) {
+                    atomicOr(A.err, ERR_NEED_FULL_F);
+                    continue;
+               }
+          }
+          emit_trigger<false>(A, b, k, (double)f);
      }
 }
 

@@ -181,6 +181,35 @@ struct StoreFourstep {
      }
 };
 
+// StoreFourstep for the FP32 spindown transform (two arrays) with the row
+// length N2 fixed at compile time (CN2 > 0, else the struct's N2) and the
+// thread's base twiddles read from global tables instead of shared copies:
+// w0[t*N2 + n2] = W^(n2*t) (t < L/8) and ws[n2] = W^(n2*L/8), forward sign,
+// formed in FP64 and rounded once.  The eight twiddles W^(n2*(t + m*L/8))
+// then follow by the same recurrence as StoreFourstep's FP32 path.
+template <int CN2 = 0>
+struct StoreFourstepG {
+     float2 *y;
+     const float2 *w0, *ws;
+     int N2;
+     int N;   // array stride (nfftf)
+
+     template <int L>
+     __device__ __forceinline__ void store(const float2 (&v)[2][8], int b, int n2, int t) const {
+          const int n2s = CN2 > 0 ? CN2 : N2;
+          float2 w = __ldg(&w0[t * n2s + n2]);
+          const float2 st = __ldg(&ws[n2]);
+          float4 *dst = reinterpret_cast<float4 *>(y) + ((size_t)b * N + n2 + (size_t)t * n2s);
+          const int step = (L / 8) * n2s;   // elements between the thread's outputs
+#pragma unroll
+          for (int m = 0; m < 8; m++) {
+               if (m > 0) w = cmul(w, st);
+               const float2 p = cmul(v[0][m], w), q = cmul(v[1][m], w);
+               dst[(size_t)m * step] = make_float4(p.x, p.y, q.x, q.y);
+          }
+     }
+};
+
 // Row-pass source: rows of Y laid out as in StoreFourstep.  load() fills the
 // first-pass inputs v[a][m] = row k1 element t + m*L/8 of every array.
 template <typename T, int NA>

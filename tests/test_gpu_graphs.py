@@ -144,3 +144,21 @@ def test_row_pass_without_bulk_copies_matches(golden, monkeypatch, name):
     eng = Engine.from_job(g.job32, form="split")
     _same(_records(eng.search(pm, mm, nn)), ref)
     eng.close()
+
+
+@pytest.mark.parametrize("name", ["g2_h1l1_inj", "g5_vlines", "g6_h1l1v1", "g7_fftpad2"])
+def test_sparse_f_store_matches_full_store(golden, monkeypatch, name):
+    """The split form's default F store (the row pass keeps F on the chip:
+    candidate records and the edge bins of its runs only) gives the same
+    records, bit for bit, as TDF_FULL_F=1 (every F spectrum written to the
+    F ring and scanned by the trigger selection)."""
+    from tdfstat_b200.engine import Engine
+    g = golden(name)
+    pm, mm, nn = g.job32.sky_points()
+    eng = Engine.from_job(g.job32, form="split")
+    ref = _records(eng.search(pm, mm, nn))
+    eng.close()
+    monkeypatch.setenv("TDF_FULL_F", "1")
+    eng = Engine.from_job(g.job32, form="split")
+    _same(_records(eng.search(pm, mm, nn)), ref)
+    eng.close()

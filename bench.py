@@ -264,7 +264,9 @@ def run_tdf(args, rank, world, local_rank):
         eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
         stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
         # chunk size by the engine's autotuner on a 16-point sample (untimed)
-        tuned = eng.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
+        if not args.no_autotune:
+            eng.autotune(pm[:16], mm[:16], nn[:16])
+        tuned = eng.tuning()
         # warm-up steps are the timed step exactly (the flush included: its
         # first launch loads torch's fill kernel)
         for k in range(args.warmup):
@@ -376,7 +378,7 @@ def run_tdf(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
                 "data": "synthetic (seeded Gaussian noise + injected CW signals, synthetic ephemeris)",
-                "config": dict(wl.config, form=args.form, templates_per_chunk=tuned,
+                "config": dict(wl.config, form=args.form, tuning=tuned,
                                step=("one %d-point slice of the %d-point patch per step, slices in turn"
                                      % (len(slices[0][0]), len(pm)) if len(slices) > 1
                                      else "the whole patch per step"),
@@ -415,7 +417,9 @@ def run_sweep(args, rank, world, local_rank):
         eng = Engine(seg, opts, form=args.form, device=local_rank, max_sky_batch=args.sky_batch)
         stream = torch.cuda.ExternalStream(eng.stream(), device=local_rank)
         flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-        tuned = eng.autotune(wl.pm[:16], wl.mm[:16], wl.nn[:16]) if not args.no_autotune else None
+        if not args.no_autotune:
+            eng.autotune(wl.pm[:16], wl.mm[:16], wl.nn[:16])
+        tuned = eng.tuning()
         peak, peak_kind = measured_peaks()
         bt = len(job.dets) * job.sett.N * (24 if args.form == "split" else 40)
         for k in range(10, 19):
@@ -436,7 +440,7 @@ def run_sweep(args, rank, world, local_rank):
                 "data": "synthetic (seeded Gaussian noise, sigma 1.0 / 1.3, 10% gaps, injected CW signal)",
                 "config": dict(wl.config, sky_points=npts, templates_per_step=npts * wl.nspd,
                                timed_sky_points=timed, templates_searched=int(nsearched),
-                               form=args.form, templates_per_chunk=tuned,
+                               form=args.form, tuning=tuned,
                                patch="%d x %d points over 3.2 x 3.2 grid cells" % (1 << (k // 2), 1 << (k - k // 2)),
                                timed=("the whole patch" if timed == npts else
                                       "the patch's first %d points (every template counted is searched)" % timed)),
@@ -450,18 +454,29 @@ def run_sweep(args, rank, world, local_rank):
 
 
 def run_tdf_segments(args, rank, world, local_rank):
-    """cfg4: 64 segments of four sizes.  One engine per size, all on one
-    stream; a step streams every segment in (tdf_engine_upload: its inputs
-    from host memory) and searches its patch.  `value` includes the uploads
-    (the data of 64 segments is not resident at once); `e2e` also brings the
-    records back (tdf_search_points)."""
+    """cfg4: 64 segments of four sizes (N = 86164, 129246, 172328, 258492),
+    each with its own inputs and a 16 x 16 patch x 401 spindowns.  A step
+    brings every segment's inputs in from host memory and searches all of
+    them.  Three ways to run the same step are timed, each with its own
+    engines (one per segment size):
+      plan        every segment of a size resident in its own slot of one
+                  engine (tdf_engine_add_segment / upload_segment) and the
+                  size's whole search one call (tdf_search_segments_device):
+                  one captured graph per segment size spanning all its
+                  segments (the line's value)
+      batch       one segment at a time in slot 0 (tdf_engine_upload), one
+                  captured graph per 8-point sky batch
+      plain       as batch with every kernel launched from the host
+                  (TDF_GRAPHS=0): one launch set per segment
+    `value` includes the uploads (the data of 64 segments is brought in
+    every step); `e2e` (batch form) also brings the records back
+    (tdf_search_points)."""
     import torch
     import torch.distributed as dist
     from tdfstat_b200.engine import Engine
 
     torch.cuda.set_device(local_rank)
     root = tempfile.mkdtemp(prefix="tdfbench4_")
-    engines = {}
     try:
         if args.segments_by_cost:
             # whole segments to ranks by estimated cost; the total work is fixed
@@ -474,95 +489,152 @@ def run_tdf_segments(args, rank, world, local_rank):
         else:
             mw = MultiWorkload(root, world=world)
             shards = [(w,) + tuple(w.shard(rank, world)) for w in mw.segments]
+        sizes = sorted({w.job.sett.N for w, _, _, _ in shards})
         # above the default priority, so that the engines' low-priority sky
         # stream fills this stream's kernel tails instead of competing
         stream = torch.cuda.Stream(device=local_rank, priority=-1)
-        tuned = {}
-        for w, pm, mm, nn in shards:
-            N = w.job.sett.N
-            if N not in engines:
-                e = Engine(w.job.segment(), w.job.search_opts(), form=args.form, device=local_rank,
-                           max_sky_batch=args.sky_batch)
-                e.set_stream(stream.cuda_stream)
-                tuned[N] = e.autotune(pm[:16], mm[:16], nn[:16]) if not args.no_autotune else None
-                engines[N] = e
         flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-        def step(records=False):
-            n = 0
-            for w, pm, mm, nn in shards:
-                e = engines[w.job.sett.N]
-                e.upload(w.job.segment())
-                n += len(e.search(pm, mm, nn)) if records else e.search_device(pm, mm, nn)[0]
-            return n
 
         def barrier():
             if world > 1:
                 dist.barrier()
 
-        for _ in range(args.warmup):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            step()
-        torch.cuda.synchronize()
-        launches0 = sum(e.launch_count() for e in engines.values())
-        clocks = ClockSampler(local_rank)
-        clocks.start()
-        barrier()
-        torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        nsearched = 0
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            nsearched += step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        clk = clocks.stop()
-        ms = ev0.elapsed_time(ev1)
-        launches = sum(e.launch_count() for e in engines.values()) - launches0
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        nsearched_e2e = 0
-        for _ in range(args.steps):
-            nsearched_e2e += step(records=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        ms_e2e = e0.elapsed_time(e1)
-        t = torch.tensor([ms, ms_e2e], dtype=torch.float64, device="cuda")
-        n = torch.tensor([nsearched, nsearched_e2e], dtype=torch.float64, device="cuda")
+        def make_engines(plain):
+            if plain:
+                os.environ["TDF_GRAPHS"] = "0"
+            try:
+                engines, tuned = {}, {}
+                for w, pm, mm, nn in shards:
+                    N = w.job.sett.N
+                    if N not in engines:
+                        e = Engine(w.job.segment(), w.job.search_opts(), form=args.form, device=local_rank,
+                                   max_sky_batch=args.sky_batch)
+                        e.set_stream(stream.cuda_stream)
+                        if not args.no_autotune:
+                            e.autotune(pm[:16], mm[:16], nn[:16])
+                        tuned[N] = e.tuning()
+                        engines[N] = e
+                return engines, tuned
+            finally:
+                os.environ.pop("TDF_GRAPHS", None)
+
+        def timed(step, steps):
+            clocks = ClockSampler(local_rank)
+            clocks.start()
+            barrier()
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            n = 0
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                n += step()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            return ev0.elapsed_time(ev1), n, clocks.stop()
+
+        res = {}
+        # ---- plan: all segments of a size resident, one call (one graph) per size
+        engines, tuned = make_engines(False)
+        slot_of, groups = {}, {N: [] for N in sizes}
+        for w, pm, mm, nn in shards:
+            e = engines[w.job.sett.N]
+            if not groups[w.job.sett.N]:
+                slot_of[id(w)] = 0
+            else:
+                slot_of[id(w)] = e.add_segment(w.job.segment())
+            groups[w.job.sett.N].append((w, pm, mm, nn))
+        calls = {}
+        for N, g in groups.items():
+            calls[N] = ([slot_of[id(w)] for w, _, _, _ in g], [len(pm) for _, pm, _, _ in g],
+                        np.concatenate([pm for _, pm, _, _ in g]), np.concatenate([mm for _, _, mm, _ in g]),
+                        np.concatenate([nn for _, _, _, nn in g]))
+
+        def step_plan():
+            n = 0
+            for N, g in groups.items():
+                e = engines[N]
+                for w, _, _, _ in g:
+                    e.upload_segment(slot_of[id(w)], w.job.segment())
+                n += e.search_segments_device(*calls[N])[0]
+            return n
+
+        for _ in range(max(args.warmup, 2)):   # the second call captures each size's graph
+            step_plan()
+        l0 = sum(e.launch_count() for e in engines.values())
+        ms, nsearched, clk = timed(step_plan, args.steps)
+        launches = sum(e.launch_count() for e in engines.values()) - l0
+        res["plan"] = (ms, nsearched)
+        tuned_plan = tuned
+        for e in engines.values():
+            e.close()
+
+        # ---- batch (graph per 8-point batch) and plain (no graphs): one segment at a time
+        def per_segment(engines, records=False):
+            def step():
+                n = 0
+                for w, pm, mm, nn in shards:
+                    e = engines[w.job.sett.N]
+                    e.upload(w.job.segment())
+                    n += len(e.search(pm, mm, nn)) if records else e.search_device(pm, mm, nn)[0]
+                return n
+            return step
+
+        e2e = None
+        for mode in ("batch", "plain"):
+            if mode == "plain" and args.no_cfg4_compare:
+                continue
+            engines, _ = make_engines(mode == "plain")
+            st = per_segment(engines)
+            for _ in range(args.warmup):
+                st()
+            ms_m, n_m, _ = timed(st, args.steps)
+            res[mode] = (ms_m, n_m)
+            if mode == "batch":
+                ms_e, n_e, _ = timed(per_segment(engines, records=True), args.steps)
+                e2e = (ms_e, n_e)
+            for e in engines.values():
+                e.close()
+
+        keys = list(res)
+        t = torch.tensor([res[k][0] for k in keys] + [e2e[0]], dtype=torch.float64, device="cuda")
+        n = torch.tensor([res[k][1] for k in keys] + [e2e[1]], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        ms, ms_e2e = float(t[0]), float(t[1])
+        vals = {k: float(n[i]) / (float(t[i]) / 1e3) for i, k in enumerate(keys)}
+        ms = float(t[0])
         h2d = sum(sum(d.xdat.nbytes + d.detssb.nbytes for d in w.job.dets) + w.job.cosmodf.nbytes +
                   w.job.sinmodf.nbytes for w, _, _, _ in shards)
         if rank != 0:
             return None
         return {
-            "metric": METRIC, "value": round(float(n[0]) / (ms / 1e3), 1), "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": round(vals["plan"], 1), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
             "higher_is_better": True, "scaling": "strong" if args.segments_by_cost else "weak",
             "vs_baseline": None,
             "dtype": "f32+f64 (split)" if args.form == "split" else "f64",
             "data": "synthetic (seeded Gaussian noise + injected CW signal per segment, synthetic ephemeris)",
-            "config": dict(mw.config, form=args.form, templates_per_chunk={str(k): v for k, v in tuned.items()},
+            "config": dict(mw.config, form=args.form, tuning={str(k): v for k, v in tuned_plan.items()},
                            distribution=("whole segments to ranks by estimated cost" if args.segments_by_cost
                                          else "every segment's sky patch split over the ranks"),
                            templates_searched_per_step=int(round(float(n[0]) / args.steps)),
-                           engines="one per segment size, segments streamed in by tdf_engine_upload each step",
+                           engines="one per segment size; value: every segment of a size resident in its own "
+                                   "slot, the size's search one captured graph; inputs of all 64 segments "
+                                   "uploaded from host memory in every step",
                            l2="flush: 256 MiB write between timed steps; per-step working set > L2"),
-            "e2e": {"value": round(float(n[1]) / (ms_e2e / 1e3), 1), "unit": UNIT,
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None},
+            "compare": {"one_graph_per_segment_size": round(vals["plan"], 1),
+                        "graph_per_8_point_batch": round(vals["batch"], 1),
+                        "plain_launches_per_segment": round(vals["plain"], 1) if "plain" in vals else None},
+            "e2e": {"value": round(float(n[-1]) / (float(t[-1]) / 1e3), 1), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": None,
+                    "form": "graph per 8-point batch, records brought back (tdf_search_points)"},
             "gpu_launches": int(launches),
             "roofline": None, "cpu_baseline": None, "clocks": clk,
         }
     finally:
-        for e in engines.values():
-            e.close()
         shutil.rmtree(root, ignore_errors=True)
 
 
@@ -622,6 +694,7 @@ def main():
                     help="cfg4 on several GPUs: whole segments to ranks by estimated cost (strong scaling)")
     ap.add_argument("--sky-points", type=int, default=0, help="use only the first K sky points (profiling runs)")
     ap.add_argument("--sweep", action="store_true", help="cfg5: one line per sky-patch size 2^10 .. 2^18")
+    ap.add_argument("--no-cfg4-compare", action="store_true", help="cfg4: skip the plain-launch comparison")
     ap.add_argument("--sweep-cap", type=int, default=4096, help="sky points timed per sweep size at most")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

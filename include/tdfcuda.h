@@ -169,6 +169,32 @@ int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const f
                              const float *nn, const float *sst,
                              int64_t *nrec, int64_t *ntrig);
 
+/* Several data segments of the same sizes resident on one engine.  The
+   reference searches one segment per process (search/network/openmp/main.c;
+   its spline keeps a static buffer sized for one N, auxi.c:97-99); here a
+   run over many segments of one length keeps them all on the GPU.
+   tdf_engine_add_segment() uploads another segment (sizes and detector count
+   equal to the engine's; its grid matrix, ephemeris, noise levels and data
+   may differ) and returns its slot (the engine's own segment is slot 0);
+   tdf_engine_upload_segment() replaces a slot's inputs;
+   tdf_engine_segment_count() gives the number of slots. */
+int tdf_engine_add_segment(tdf_engine *e, const tdf_segment *seg, int32_t *slot);
+int tdf_engine_upload_segment(tdf_engine *e, int32_t slot, const tdf_segment *seg);
+int tdf_engine_segment_count(tdf_engine *e, int32_t *count);
+
+/* Device-only pass over the points of several resident segments: segment
+   slots[k] searches npts[k] points (pm, mm, nn hold them one segment after
+   the other; spindowns from spndr[0]), the work of that many job_core()
+   calls per segment (jobcore.c:193-630).  All template parameters are
+   formed and uploaded first and the call's whole device work -- every
+   batch's sky stage and spindown stage, segment after segment -- is one
+   enqueue sequence with no host step between batches; the second call with
+   the same batch list captures it into one CUDA graph, later calls replay
+   it with a single launch.  Returns the record and trigger counts. */
+int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots, const int32_t *npts,
+                               const int32_t *pm, const float *mm, const float *nn,
+                               int64_t *nrec, int64_t *ntrig);
+
 /* The full F-statistic of one template (sky point, spindown ss) over bins
    [fr0, fr1], after the optional blocks_avg normalisation: F[k - fr0]
    (jobcore.c:481-515).  Returns TDF_ERR_INVALID if the point is outside the
@@ -304,13 +330,19 @@ int tdf_fstat_operands_static(const void *d_xab, const float *d_s2, int32_t nifo
 int tdf_engine_get_stream(tdf_engine *e, void **stream);
 int tdf_engine_set_stream(tdf_engine *e, void *stream);
 
-/* Chooses the templates per chunk of the spindown stage by timing a few
-   sizes (6..48) on these points (device-only passes) and keeps the fastest
-   in the engine; *best (may be NULL) receives it.  With the environment
-   variable TDF_AUTOTUNE_CACHE=<file> the choice is appended to that file and
-   picked up by engines created later for the same form, sizes and GPU. */
+/* Chooses the spindown stage's launch configuration by timing device-only
+   passes over these points: the templates per chunk (one column-pass and
+   one row-pass launch each; 6..48), then the lanes (concurrent streams with
+   their own buffers; 2..4), then the templates per resolve group (the
+   trigger-selection launch's share; 32, 64, 128), each at the best of the
+   previous choices, and keeps the fastest in the engine; *best (may be
+   NULL) receives the templates per chunk, tdf_engine_get_tuning() all
+   three.  With the environment variable TDF_AUTOTUNE_CACHE=<file> the
+   choice is appended to that file and picked up by engines created later
+   for the same form, sizes, GPU, sky batch and F store. */
 int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
                         int32_t *best);
+int tdf_engine_get_tuning(tdf_engine *e, int32_t *templates_per_chunk, int32_t *lanes, int32_t *group_templates);
 
 /* Templates per chunk of the spindown stage (one column-pass and one
    row-pass launch each): get, and set to 1..48 (TDF_ERR_INVALID otherwise).

@@ -182,6 +182,11 @@ ABI_FUNCTIONS = [
     ("tdf_last_results", C.c_int, [P, RECP, C.c_int64, I64P, F32P, C.c_int64, I64P, I32P]),
     ("tdf_search_points_device", C.c_int,
      [P, C.c_int, I32P, F32P, F32P, F32P, I64P, I64P]),
+    ("tdf_engine_add_segment", C.c_int, [P, C.POINTER(TdfSegment), I32P]),
+    ("tdf_engine_get_tuning", C.c_int, [P, I32P, I32P, I32P]),
+    ("tdf_engine_upload_segment", C.c_int, [P, C.c_int32, C.POINTER(TdfSegment)]),
+    ("tdf_engine_segment_count", C.c_int, [P, I32P]),
+    ("tdf_search_segments_device", C.c_int, [P, C.c_int32, I32P, I32P, I32P, F32P, F32P, I64P, I64P]),
     ("tdf_fstat_spectrum", C.c_int,
      [P, C.c_int32, C.c_float, C.c_float, C.c_float, F64P, C.c_int64]),
     ("tdf_engine_add_signal", C.c_int, [P, C.POINTER(TdfSignal), F64P, I32P]),

@@ -269,6 +269,17 @@ struct HostPoint {
      int first_tmpl = 0;
 };
 
+// The inputs of one data segment resident on the engine's GPU: the host
+// scalars the per-point set-up reads and the device copies the sky stage
+// reads.  Slot 0 is the segment the engine was created with; further
+// segments of the same sizes may be added (tdf_engine_add_segment).
+struct SegData {
+     tdf_segment seg{};
+     std::vector<DetParam> dets;
+     DevBuf xdat, detssb, cosm, sinm, detp;
+     void release() { xdat.release(); detssb.release(); cosm.release(); sinm.release(); detp.release(); }
+};
+
 struct tdf_engine {
      int dev = 0, form = TDF_FORM_SPLIT;
      cudaStream_t own = nullptr, stream = nullptr;
@@ -286,21 +297,24 @@ struct tdf_engine {
      int prio_low = 0, prio_high = 0;     // the device's stream priority range (low >= high numerically)
      bool stream_outranks_sky = true;     // the engine stream has a higher priority than sky_stream
      cudaEvent_t sky_done[2] = {nullptr, nullptr}, spin_done[2] = {nullptr, nullptr};
-     tdf_segment seg{};
+     std::vector<SegData> sdv;   // resident segments; the work being enqueued reads sdv[act]
+     int act = 0;
+     SegData &S() { return sdv[act]; }
+     const SegData &S() const { return sdv[act]; }
      tdf_search_opts opts{};
      std::vector<double> lines;
-     std::vector<DetParam> dets;
      int N = 0, nfft = 0, nfftf = 0, Ninterp = 0, nifo = 0, Nal = 0, n2N = 0;
      int nF = 0, nblk_mu = 0;
      int Bs = 8;        // sky points per batch
      int Tc = 16;       // templates per chunk (intermediate spectra sized for L2)
      int TcMax = 32;    // buffers are sized for chunks up to this size
      int Gt = 64;       // templates per resolve group at most (whole chunks; TDF_GROUP_TEMPLATES)
+     static constexpr int kGtMax = 128;   // buffers are sized for groups up to this size
      int64_t launches = 0;
      FFTTables<double> t_nfft, t_ninterp, t_f64;
      FFTTables<float> t_f32;
      // inputs
-     DevBuf xdat, detssb, cosm, sinm, pco, gco, detp;
+     DevBuf pco, gco;
      // sky stage
      DevBuf skyp[2], B0, B1, B2, shftf, partial, aabb[2];
      // operands
@@ -366,6 +380,19 @@ struct tdf_engine {
      };
      static constexpr size_t kMaxGraphs = 8;
      std::vector<GraphEntry> graphs;
+     // whole-call plans (tdf_search_segments_device): every batch's sky and
+     // template parameters on the device at once, the call's work captured
+     // as one graph, keyed by a hash of its batch list and configuration
+     DevBuf plan_sky, plan_tp;
+     cudaEvent_t plan_ev = nullptr;
+     struct PlanGraph {
+          uint64_t key = 0;
+          int seen = 0;
+          cudaGraphExec_t exec = nullptr;
+          int64_t launches = 0;
+          uint64_t last = 0;
+     };
+     std::vector<PlanGraph> plan_graphs;
      uint64_t graph_tick = 0;
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
      bool row_bulk = true;     // row passes fetch their rows by bulk copies (TDF_ROW_BULK=0: per thread)
@@ -465,20 +492,20 @@ static int validate(const tdf_segment *s, const tdf_search_opts *o) {
 static int upload_inputs(tdf_engine *e, const tdf_segment *s) {
      const int N = e->N, nifo = e->nifo;
      for (int d = 0; d < nifo; d++) {
-          CUCHK(cudaMemcpyAsync(e->xdat.as<float>() + (size_t)d * e->Nal, s->det[d].xdat, N * sizeof(float),
+          CUCHK(cudaMemcpyAsync(e->S().xdat.as<float>() + (size_t)d * e->Nal, s->det[d].xdat, N * sizeof(float),
                                 cudaMemcpyHostToDevice, e->stream));
-          CUCHK(cudaMemcpyAsync(e->detssb.as<double>() + (size_t)d * 3 * N, s->det[d].detssb, 3 * (size_t)N * sizeof(double),
+          CUCHK(cudaMemcpyAsync(e->S().detssb.as<double>() + (size_t)d * 3 * N, s->det[d].detssb, 3 * (size_t)N * sizeof(double),
                                 cudaMemcpyHostToDevice, e->stream));
-          DetParam &D = e->dets[d];
+          DetParam &D = e->S().dets[d];
           for (int k = 0; k < 9; k++) D.amod[k] = s->det[d].amod[k];
           D.cphir = s->det[d].cphir;
           D.sphir = s->det[d].sphir;
           D.sig2 = s->det[d].sig2;
      }
-     CUCHK(cudaMemcpyAsync(e->cosm.p, s->cosmodf, N * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-     CUCHK(cudaMemcpyAsync(e->sinm.p, s->sinmodf, N * sizeof(double), cudaMemcpyHostToDevice, e->stream));
-     CUCHK(cudaMemcpyAsync(e->detp.p, e->dets.data(), nifo * sizeof(DetParam), cudaMemcpyHostToDevice, e->stream));
-     e->seg = *s;
+     CUCHK(cudaMemcpyAsync(e->S().cosm.p, s->cosmodf, N * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+     CUCHK(cudaMemcpyAsync(e->S().sinm.p, s->sinmodf, N * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+     CUCHK(cudaMemcpyAsync(e->S().detp.p, e->S().dets.data(), nifo * sizeof(DetParam), cudaMemcpyHostToDevice, e->stream));
+     e->S().seg = *s;
      return TDF_OK;
 }
 
@@ -567,15 +594,23 @@ static int staged_setup(tdf_engine *e) {
      return TDF_OK;
 }
 
+// device inputs of one resident segment (xDat rows padded to Nal with zeros)
+static int seg_alloc(const tdf_engine *e, SegData &d) {
+     const int nifo = e->nifo;
+     d.dets.resize(nifo);
+     TRY(d.xdat.alloc((size_t)nifo * e->Nal * sizeof(float)));
+     CUCHK(cudaMemset(d.xdat.p, 0, d.xdat.bytes));
+     TRY(d.detssb.alloc((size_t)nifo * 3 * e->N * sizeof(double)));
+     TRY(d.cosm.alloc(e->N * sizeof(double)));
+     TRY(d.sinm.alloc(e->N * sizeof(double)));
+     TRY(d.detp.alloc(nifo * sizeof(DetParam)));
+     return TDF_OK;
+}
+
 static int engine_alloc(tdf_engine *e) {
      const int nifo = e->nifo, Bs = e->Bs, Tc = e->TcMax;
      const size_t Q = (size_t)Bs * nifo;
-     TRY(e->xdat.alloc((size_t)nifo * e->Nal * sizeof(float)));
-     CUCHK(cudaMemset(e->xdat.p, 0, e->xdat.bytes));
-     TRY(e->detssb.alloc((size_t)nifo * 3 * e->N * sizeof(double)));
-     TRY(e->cosm.alloc(e->N * sizeof(double)));
-     TRY(e->sinm.alloc(e->N * sizeof(double)));
-     TRY(e->detp.alloc(nifo * sizeof(DetParam)));
+     TRY(seg_alloc(e, e->sdv[0]));
      // spline recurrence factors (auxi.c:102-108): invp[i] = 2/(g[i-1]+4), g[i] = -0.5 invp[i]
      {
           const int n = e->n2N;
@@ -612,9 +647,9 @@ static int engine_alloc(tdf_engine *e) {
      }
      const size_t csz = e->form == TDF_FORM_SPLIT ? sizeof(float2) : sizeof(double2);
      const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
-     const size_t G = (size_t)std::max(e->Gt, Tc);   // templates per resolve group at most
+     const size_t G = (size_t)std::max(tdf_engine::kGtMax, Tc);   // templates per resolve group at most
      e->cand_cap = (unsigned)G * 4096u;
-     for (int l = 0; l < e->nlanes; l++) {
+     for (int l = 0; l < tdf_engine::kMaxLanes; l++) {   // every lane: the autotuner may use them all
           tdf_engine::Lane &L = e->ln[l];
           TRY(L.Ybuf.alloc((size_t)Tc * 2 * e->nfftf * csz));
           TRY(L.Fbuf.alloc(G * e->nF * rsz));
@@ -652,11 +687,15 @@ static void graphs_clear(tdf_engine *e) {
      for (auto &g : e->graphs)
           if (g.exec) cudaGraphExecDestroy(g.exec);
      e->graphs.clear();
+     for (auto &g : e->plan_graphs)
+          if (g.exec) cudaGraphExecDestroy(g.exec);
+     e->plan_graphs.clear();
 }
 
 static void engine_free(tdf_engine *e) {
      graphs_clear(e);
-     DevBuf *bufs[] = {&e->xdat, &e->detssb, &e->cosm, &e->sinm, &e->pco, &e->gco, &e->detp, &e->skyp[0],
+     for (SegData &d : e->sdv) d.release();
+     DevBuf *bufs[] = {&e->pco, &e->gco, &e->plan_sky, &e->plan_tp, &e->skyp[0],
                        &e->skyp[1], &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb[0], &e->aabb[1],
                        &e->xab[0], &e->xab[1], &e->s2[0], &e->s2[1], &e->xa64[0], &e->xa64[1], &e->xb64[0],
                        &e->xb64[1], &e->t1[0], &e->t1[1], &e->tparam, &e->trig[0], &e->trig[1],
@@ -695,6 +734,8 @@ static void engine_free(tdf_engine *e) {
      }
      if (e->fork_ev) cudaEventDestroy(e->fork_ev);
      e->fork_ev = nullptr;
+     if (e->plan_ev) cudaEventDestroy(e->plan_ev);
+     e->plan_ev = nullptr;
      for (int l = 0; l < tdf_engine::kMaxLanes; l++) {
           if (e->join_ev[l]) cudaEventDestroy(e->join_ev[l]);
           if (e->lane_own[l]) cudaStreamDestroy(e->lane_own[l]);
@@ -712,16 +753,16 @@ static void engine_free(tdf_engine *e) {
 // jobcore.c:243-262 (sky geometry) and 399-430 (spindown range), with the
 // reference's float/double types; `flt` selects FLOAT_TYPE = float.
 static void point_setup(const tdf_engine *e, int pm, float mm, float nn, float sst, HostPoint &P) {
-     const double *M = e->seg.M;
+     const double *M = e->S().seg.M;
      double al1 = nn * M[10] + mm * M[14];
      double al2 = nn * M[11] + mm * M[15];
-     double cof = e->seg.oms;
+     double cof = e->S().seg.oms;
      P.inside = !(((al1 * al1) + (al2 * al2)) / (cof * cof) > 1.);
      if (!P.inside) return;
      double be1 = al1 / cof, be2 = al2 / cof;
-     double sindel = be1 * e->seg.sepsm - (2 * pm - 3) * std::sqrt(1. - be1 * be1 - be2 * be2) * e->seg.cepsm;
+     double sindel = be1 * e->S().seg.sepsm - (2 * pm - 3) * std::sqrt(1. - be1 * be1 - be2 * be2) * e->S().seg.cepsm;
      double cosdel = std::sqrt(1. - sindel * sindel);
-     double sinal = (be1 - e->seg.sepsm * sindel) / (e->seg.cepsm * cosdel);
+     double sinal = (be1 - e->S().seg.sepsm * sindel) / (e->S().seg.cepsm * cosdel);
      double cosal = be2 / cosdel;
      SkyParam &S = P.sp;
      S.sinalt = sinal;
@@ -737,8 +778,8 @@ static void point_setup(const tdf_engine *e, int pm, float mm, float nn, float s
      P.ra = (float)std::fmod(std::atan2(sinal, cosal) + 2. * M_PI, 2. * M_PI);
      float smin = sst, smax = e->opts.spndr[1];
      if (e->opts.allsky) {
-          smin = std::trunc((e->seg.Smin - nn * M[9] - mm * M[13]) / M[5]);
-          smax = std::trunc(-(nn * M[9] + mm * M[13] + e->seg.Smax) / M[5]);
+          smin = std::trunc((e->S().seg.Smin - nn * M[9] - mm * M[13]) / M[5]);
+          smax = std::trunc(-(nn * M[9] + mm * M[13] + e->S().seg.Smax) / M[5]);
           if (smin > smax) {
                smin = smin + smax;
                smax = smin - smax;
@@ -753,7 +794,7 @@ static void point_setup(const tdf_engine *e, int pm, float mm, float nn, float s
 }
 
 static void tmpl_setup(const tdf_engine *e, const HostPoint &P, float mm, float nn, float ss, HostTmpl &T) {
-     const double *M = e->seg.M;
+     const double *M = e->S().seg.M;
      T.ss = ss;
      T.spnd = ss * M[5] + nn * M[9] + mm * M[13];
      double het1 = std::fmod(ss * M[4], M[0]);
@@ -772,8 +813,8 @@ static void tmpl_setup(const tdf_engine *e, const HostPoint &P, float mm, float 
 
 // fdot of the record (jobcore.c:439,447): sgnlt[1] is FLOAT_TYPE
 static float rec_fdot(const tdf_engine *e, double spnd) {
-     if (e->form == TDF_FORM_SPLIT) return (float)((double)(float)spnd / (M_PI * e->seg.dt * e->seg.dt));
-     return (float)(spnd / (M_PI * e->seg.dt * e->seg.dt));
+     if (e->form == TDF_FORM_SPLIT) return (float)((double)(float)spnd / (M_PI * e->S().seg.dt * e->S().seg.dt));
+     return (float)(spnd / (M_PI * e->S().seg.dt * e->S().seg.dt));
 }
 
 // ------------------------------------------------------------------ device pipeline
@@ -791,23 +832,29 @@ static cudaStream_t sky_stream_of(const tdf_engine *e) {
 // Sky stage of npts points into batch slot e->cur, on the sky stream: it
 // first waits until the slot's previous spindown work released the slot's
 // operands, and records sky_done[slot] for the spindown work to wait on.
-static int run_sky_stage(tdf_engine *e, int npts) {
+// dsky: the points' sky parameters already on the device (else the slot's
+// pinned staging is copied); wait_on: the event the sky stream waits for
+// before it overwrites the slot (default: the slot's previous spindown work).
+static int run_sky_stage(tdf_engine *e, int npts, const SkyParam *dsky = nullptr, cudaEvent_t wait_on = nullptr) {
      e->signal_valid = false;   // B0 is the sky stage's work buffer
      cudaStream_t st = sky_stream_of(e);
-     CUCHK(cudaStreamWaitEvent(st, e->spin_done[e->cur], 0));
+     CUCHK(cudaStreamWaitEvent(st, wait_on ? wait_on : e->spin_done[e->cur], 0));
      const int nifo = e->nifo, Q = npts * nifo;
      const size_t ws = Wstride(e);
      const int sl = e->cur;
-     CUCHK(cudaMemcpyAsync(e->skyp[sl].p, e->h_sky[sl], npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
+     if (!dsky) {
+          CUCHK(cudaMemcpyAsync(e->skyp[sl].p, e->h_sky[sl], npts * sizeof(SkyParam), cudaMemcpyHostToDevice, st));
+          dsky = e->skyp[sl].as<SkyParam>();
+     }
      const int nblk = e->nfft / 256;
      const bool split = e->form == TDF_FORM_SPLIT;
      k_sky_prep<<<dim3(nblk, Q), 256, 0, st>>>(
-          e->xdat.as<float>(), e->detssb.as<double>(), e->cosm.as<double>(), e->sinm.as<double>(),
-          e->skyp[sl].as<SkyParam>(), e->detp.as<DetParam>(), nifo, e->N, e->nfft, e->Nal, e->seg.oms,
+          e->S().xdat.as<float>(), e->S().detssb.as<double>(), e->S().cosm.as<double>(), e->S().sinm.as<double>(),
+          dsky, e->S().detp.as<DetParam>(), nifo, e->N, e->nfft, e->Nal, e->S().seg.oms,
           e->B0.as<double2>(), ws, e->shftf.as<double>(), split ? e->s2[sl].as<float>() : nullptr,
           split ? nullptr : e->t1[sl].as<double>(), e->partial.as<double>());
      CUCHK(cudaGetLastError());
-     k_sky_sums<<<npts, 256, 0, st>>>(e->partial.as<double>(), nblk, e->detp.as<DetParam>(), nifo,
+     k_sky_sums<<<npts, 256, 0, st>>>(e->partial.as<double>(), nblk, e->S().detp.as<DetParam>(), nifo,
                                        e->aabb[sl].as<AaBb>());
      CUCHK(cudaGetLastError());
      e->launches += 2;
@@ -829,7 +876,7 @@ static int run_sky_stage(tdf_engine *e, int npts) {
           StoreFourstep<double, +1, 1> epi{e->B1.as<double2>(), t.h(), t.o(), t.N2, (int)ws};
           TRY((launch_col<double, +1, 1>(t.N1, dim3(t.N2 / LINES, 2 * Q), pro, epi, t.l1(), st)));
           RowsY<double, 1> src{e->B1.as<double2>(), (int)ws, t.N2};
-          const double ft = (double)e->seg.interpftpad / e->Ninterp;
+          const double ft = (double)e->S().seg.interpftpad / e->Ninterp;
           StoreNatural<double> epi2{e->B0.as<double2>(), t.N1, (int)ws, e->n2N, ft};
           TRY((launch_row<double, +1, 1>(t.N2, dim3(t.N1 / LINES, 2 * Q), src, epi2, t.l2(), st)));
      }
@@ -846,7 +893,7 @@ static int run_sky_stage(tdf_engine *e, int npts) {
      }
      k_splint<<<dim3((e->N + 255) / 256, Q), 256, 0, st>>>(
           e->B0.as<double2>(), e->B2.as<double2>(), ws, e->shftf.as<double>(), e->Nal, e->N, e->n2N,
-          e->seg.interpftpad, e->detp.as<DetParam>(), nifo, split ? e->xab[sl].as<float4>() : nullptr,
+          e->S().seg.interpftpad, e->S().detp.as<DetParam>(), nifo, split ? e->xab[sl].as<float4>() : nullptr,
           split ? nullptr : e->xa64[sl].as<double2>(), split ? nullptr : e->xb64[sl].as<double2>());
      CUCHK(cudaGetLastError());
      e->launches += 3;
@@ -1218,7 +1265,7 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
           CUCHK(cudaStreamSynchronize(e->sky_stream));
           CUCHK(cudaStreamSynchronize(e->stream));
           for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
-          for (int l = 0; l < e->nlanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+          for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
           int pending[2] = {0, 0};
           bool over = false, need_full = false;
           size_t b = 0;
@@ -1315,9 +1362,12 @@ static int sm_count(int dev) {
      return n;
 }
 
+// the cache key: form, sizes, GPU (SM count), sky batch and F store; the
+// value: templates per chunk, lanes, templates per resolve group
 static std::string autotune_key(const tdf_engine *e) {
      char k[256];
-     snprintf(k, sizeof(k), "tc %d %d %d %d %d %d", e->form, e->N, e->nfftf, e->nifo, sm_count(e->dev), e->Bs);
+     snprintf(k, sizeof(k), "tune %d %d %d %d %d %d %d", e->form, e->N, e->nfftf, e->nifo, sm_count(e->dev), e->Bs,
+              e->sparse_f ? 1 : 0);
      return k;
 }
 
@@ -1330,8 +1380,13 @@ static void autotune_cache_lookup(tdf_engine *e) {
      char line[512];
      while (fgets(line, sizeof(line), f)) {
           if (strncmp(line, key.c_str(), key.size()) == 0 && line[key.size()] == ' ') {
-               int tc = atoi(line + key.size() + 1);
-               if (tc > 0 && tc <= e->TcMax) e->Tc = tc;
+               int tc = 0, lanes = 0, gt = 0;
+               if (sscanf(line + key.size() + 1, "%d %d %d", &tc, &lanes, &gt) == 3 && tc > 0 && tc <= e->TcMax &&
+                   lanes >= 1 && lanes <= tdf_engine::kMaxLanes && gt >= 1 && gt <= tdf_engine::kGtMax) {
+                    e->Tc = tc;
+                    e->nlanes = lanes;
+                    e->Gt = gt;
+               }
           }
      }
      fclose(f);
@@ -1342,7 +1397,7 @@ static void autotune_cache_store(const tdf_engine *e) {
      if (!path || !*path) return;
      FILE *f = fopen(path, "a");
      if (!f) return;
-     fprintf(f, "%s %d\n", autotune_key(e).c_str(), e->Tc);
+     fprintf(f, "%s %d %d %d\n", autotune_key(e).c_str(), e->Tc, e->nlanes, e->Gt);
      fclose(f);
 }
 
@@ -1361,6 +1416,104 @@ __global__ void k_wait_probe(unsigned *err, int probes) {
      if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);
      const bool done = mbar_wait(&bar, 0u, probes);
      if (!done && threadIdx.x == 0) atomicOr(err, ERR_STAGE_TIMEOUT);
+}
+
+// ------------------------------------------------------------------ whole-call plans
+//
+// tdf_search_segments_device(): the points of several resident segments
+// searched by one enqueue sequence -- every batch's sky stage and spindown
+// stage, segment after segment, with no host work between batches -- which
+// the second call with the same batch list captures into one CUDA graph and
+// later calls replay with a single launch.  Trigger counts accumulate in the
+// two batch slots' counters and are read once at the end.
+
+struct PlanBatch {
+     int slot, nb, nt;
+     size_t sky_off, tp_off;
+};
+
+static uint64_t fnv1a(uint64_t h, const void *p, size_t n) {
+     const unsigned char *c = (const unsigned char *)p;
+     for (size_t i = 0; i < n; i++) {
+          h ^= c[i];
+          h *= 1099511628211ull;
+     }
+     return h;
+}
+
+static int enqueue_plan(tdf_engine *e, const std::vector<PlanBatch> &pb) {
+     const SkyParam *dsky = e->plan_sky.as<SkyParam>();
+     const TmplParam *dtp = e->plan_tp.as<TmplParam>();
+     for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
+     for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+     // the sky stream's first work of the plan follows this point of the engine stream
+     CUCHK(cudaEventRecord(e->plan_ev, e->stream));
+     for (size_t i = 0; i < pb.size(); i++) {
+          e->cur = (int)(i & 1);
+          e->act = pb[i].slot;
+          const int st = run_sky_stage(e, pb[i].nb, dsky + pb[i].sky_off, i < 2 ? e->plan_ev : nullptr);
+          e->act = 0;
+          TRY(st);
+          CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[e->cur], 0));
+          TRY(run_templates(e, dtp + pb[i].tp_off, pb[i].nt));
+          CUCHK(cudaEventRecord(e->spin_done[e->cur], e->stream));
+     }
+     for (int s = 0; s < 2; s++)
+          CUCHK(cudaMemcpyAsync(e->h_cnt + 2 * s, e->counters[s].p, 2 * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, e->stream));
+     return TDF_OK;
+}
+
+// runs the plan once: the captured graph when one exists for `key`, else
+// plain launches (the first sighting) or a capture (the second)
+static int run_plan(tdf_engine *e, const std::vector<PlanBatch> &pb, uint64_t key) {
+     if (!e->use_graphs || e->timing) return enqueue_plan(e, pb);
+     size_t gi = e->plan_graphs.size();
+     for (size_t i = 0; i < e->plan_graphs.size(); i++)
+          if (e->plan_graphs[i].key == key) gi = i;
+     if (gi == e->plan_graphs.size()) {
+          if (e->plan_graphs.size() >= tdf_engine::kMaxGraphs) {
+               size_t old = 0;
+               for (size_t i = 1; i < e->plan_graphs.size(); i++)
+                    if (e->plan_graphs[i].last < e->plan_graphs[old].last) old = i;
+               if (e->plan_graphs[old].exec) cudaGraphExecDestroy(e->plan_graphs[old].exec);
+               e->plan_graphs.erase(e->plan_graphs.begin() + old);
+          }
+          e->plan_graphs.push_back(tdf_engine::PlanGraph());
+          gi = e->plan_graphs.size() - 1;
+          e->plan_graphs[gi].key = key;
+     }
+     tdf_engine::PlanGraph &g = e->plan_graphs[gi];
+     g.last = ++e->graph_tick;
+     if (!g.exec && ++g.seen < 2) return enqueue_plan(e, pb);
+     if (!g.exec) {
+          if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+               cudaGetLastError();
+               e->use_graphs = false;
+               return enqueue_plan(e, pb);
+          }
+          const int64_t l0 = e->launches;
+          const int st = enqueue_plan(e, pb);
+          cudaGraph_t graph = nullptr;
+          const cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+          if (st != TDF_OK || ce != cudaSuccess) {
+               if (graph) cudaGraphDestroy(graph);
+               e->launches = l0;
+               return st != TDF_OK ? st : set_error(TDF_ERR_CUDA, "stream capture: %s", cudaGetErrorString(ce));
+          }
+          const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+          cudaGraphDestroy(graph);
+          if (ie != cudaSuccess) {
+               g.exec = nullptr;
+               e->launches = l0;
+               return set_error(TDF_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ie));
+          }
+          g.launches = e->launches - l0;
+          e->launches = l0;
+     }
+     CUCHK(cudaGraphLaunch(g.exec, e->stream));
+     e->launches += g.launches;
+     return TDF_OK;
 }
 
 // ------------------------------------------------------------------ C ABI
@@ -1440,7 +1593,9 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      tdf_engine *e = new tdf_engine();
      e->dev = device;
      e->form = form;
-     e->seg = *seg;
+     e->sdv.resize(1);
+     e->act = 0;
+     e->S().seg = *seg;
      e->opts = *opts;
      e->N = seg->N;
      e->nfft = seg->nfft;
@@ -1468,11 +1623,11 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      const char *rb = getenv("TDF_ROW_BULK");
      if (rb && rb[0] == '0') e->row_bulk = false;
      const char *gt = getenv("TDF_GROUP_TEMPLATES");
-     if (gt && atoi(gt) > 0) e->Gt = atoi(gt);
+     if (gt && atoi(gt) > 0) e->Gt = std::min(atoi(gt), (int)tdf_engine::kGtMax);
      autotune_cache_lookup(e);
      e->lines.assign(opts->lines, opts->lines + 2 * (size_t)opts->numlines);
      e->opts.lines = nullptr;
-     e->dets.resize(seg->nifo);
+     e->S().dets.resize(seg->nifo);
      int st = TDF_OK;
      int &prio_low = e->prio_low, &prio_high = e->prio_high;
      cudaError_t ce = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
@@ -1480,7 +1635,8 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->own, cudaStreamNonBlocking, prio_high);
      if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->sky_stream, cudaStreamNonBlocking, prio_low);
      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
-     for (int l = 1; l < e->nlanes && ce == cudaSuccess; l++) {
+     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->plan_ev, cudaEventDisableTiming);
+     for (int l = 1; l < tdf_engine::kMaxLanes && ce == cudaSuccess; l++) {
           ce = cudaStreamCreateWithPriority(&e->lane_own[l], cudaStreamNonBlocking, prio_high);
           if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join_ev[l], cudaEventDisableTiming);
      }
@@ -1637,6 +1793,168 @@ int tdf_search_points_device(tdf_engine *e, int npts, const int32_t *pm, const f
      return TDF_OK;
 }
 
+int tdf_engine_add_segment(tdf_engine *e, const tdf_segment *seg, int32_t *slot) {
+     if (!e || !seg || !slot) return set_error(TDF_ERR_INVALID, "null engine, segment or slot");
+     tdf_search_opts o = e->opts;
+     o.lines = e->lines.data();
+     TRY(validate(seg, &o));
+     if (seg->N != e->N || seg->nfft != e->nfft || seg->nfftf != e->nfftf || seg->Ninterp != e->Ninterp ||
+         seg->nifo != e->nifo || seg->interpftpad != e->S().seg.interpftpad)
+          return set_error(TDF_ERR_INVALID, "segment sizes differ from the engine's");
+     if (e->sdv.size() >= 4096) return set_error(TDF_ERR_UNSUPPORTED, "at most 4096 resident segments");
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->sky_stream));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     e->sdv.emplace_back();
+     const int k = (int)e->sdv.size() - 1;
+     int st = seg_alloc(e, e->sdv[k]);
+     if (st == TDF_OK) {
+          e->act = k;
+          st = upload_inputs(e, seg);
+          e->act = 0;
+     }
+     if (st == TDF_OK) {
+          const cudaError_t ce = cudaStreamSynchronize(e->stream);
+          if (ce != cudaSuccess) st = set_error(TDF_ERR_CUDA, "segment upload: %s", cudaGetErrorString(ce));
+     }
+     if (st != TDF_OK) {
+          e->sdv[k].release();
+          e->sdv.pop_back();
+          return st;
+     }
+     *slot = k;
+     return TDF_OK;
+}
+
+int tdf_engine_upload_segment(tdf_engine *e, int32_t slot, const tdf_segment *seg) {
+     if (!e || !seg) return set_error(TDF_ERR_INVALID, "null engine or segment");
+     if (slot < 0 || slot >= (int)e->sdv.size()) return set_error(TDF_ERR_INVALID, "segment slot %d of %d", slot, (int)e->sdv.size());
+     tdf_search_opts o = e->opts;
+     o.lines = e->lines.data();
+     TRY(validate(seg, &o));
+     if (seg->N != e->N || seg->nfft != e->nfft || seg->nfftf != e->nfftf || seg->Ninterp != e->Ninterp ||
+         seg->nifo != e->nifo)
+          return set_error(TDF_ERR_INVALID, "segment sizes differ from the engine's");
+     CUCHK(cudaSetDevice(e->dev));
+     CUCHK(cudaStreamSynchronize(e->sky_stream));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     if (slot == 0) e->signal_valid = false;
+     e->act = slot;
+     const int st = upload_inputs(e, seg);
+     e->act = 0;
+     TRY(st);
+     CUCHK(cudaStreamSynchronize(e->stream));
+     return TDF_OK;
+}
+
+int tdf_engine_segment_count(tdf_engine *e, int32_t *count) {
+     if (!e || !count) return set_error(TDF_ERR_INVALID, "null argument");
+     *count = (int32_t)e->sdv.size();
+     return TDF_OK;
+}
+
+int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots, const int32_t *npts,
+                               const int32_t *pm, const float *mm, const float *nn, int64_t *nrec, int64_t *ntrig) {
+     if (!e || !nrec || !ntrig) return set_error(TDF_ERR_INVALID, "null engine or count pointers");
+     if (nseg < 0 || (nseg > 0 && (!slots || !npts))) return set_error(TDF_ERR_INVALID, "bad segment arrays");
+     int64_t tot = 0;
+     for (int k = 0; k < nseg; k++) {
+          if (slots[k] < 0 || slots[k] >= (int)e->sdv.size())
+               return set_error(TDF_ERR_INVALID, "segment slot %d of %d", slots[k], (int)e->sdv.size());
+          if (npts[k] < 0) return set_error(TDF_ERR_INVALID, "npts[%d] < 0", k);
+          tot += npts[k];
+     }
+     if (tot > 0 && (!pm || !mm || !nn)) return set_error(TDF_ERR_INVALID, "null sky point arrays");
+     CUCHK(cudaSetDevice(e->dev));
+     // the batch list: each segment's inside points in batches of Bs, with
+     // the sky and template parameters as search_core forms them
+     std::vector<PlanBatch> pb;
+     std::vector<SkyParam> hs;
+     std::vector<TmplParam> ht;
+     int64_t ntm = 0;
+     size_t off = 0;
+     for (int k = 0; k < nseg; k++) {
+          e->act = slots[k];
+          std::vector<HostPoint> pts(npts[k]);
+          std::vector<int> inside;
+          for (int i = 0; i < npts[k]; i++) {
+               const size_t q = off + i;
+               if (pm[q] != 1 && pm[q] != 2) {
+                    e->act = 0;
+                    return set_error(TDF_ERR_INVALID, "pm[%lld]=%d (must be 1 or 2)", (long long)q, pm[q]);
+               }
+               point_setup(e, pm[q], mm[q], nn[q], e->opts.spndr[0], pts[i]);
+               if (pts[i].inside && pts[i].iss_size > 0) inside.push_back(i);
+          }
+          for (size_t b0 = 0; b0 < inside.size(); b0 += e->Bs) {
+               PlanBatch B;
+               B.slot = slots[k];
+               B.nb = (int)std::min<size_t>(e->Bs, inside.size() - b0);
+               B.sky_off = hs.size();
+               B.tp_off = ht.size();
+               B.nt = 0;
+               for (int j = 0; j < B.nb; j++) {
+                    const int ip = inside[b0 + j];
+                    const HostPoint &P = pts[ip];
+                    hs.push_back(P.sp);
+                    for (int s2 = 0; s2 < P.iss_size; s2++) {
+                         HostTmpl T;
+                         tmpl_setup(e, P, mm[off + ip], nn[off + ip], P.smin + s2 * e->opts.sstep, T);
+                         TmplParam q;
+                         q.het1 = T.het1;
+                         q.spnd = T.spnd;
+                         q.sgnl0 = T.sgnl0;
+                         q.slot = j;
+                         q.id = (uint32_t)(ntm++);
+                         ht.push_back(q);
+                    }
+                    B.nt += P.iss_size;
+               }
+               pb.push_back(B);
+          }
+          off += npts[k];
+     }
+     e->act = 0;
+     if (ntm > (int64_t)UINT32_MAX) return set_error(TDF_ERR_UNSUPPORTED, "more than 2^32 templates in one call");
+     *nrec = ntm;
+     *ntrig = 0;
+     if (pb.empty()) return TDF_OK;
+     CUCHK(cudaStreamSynchronize(e->sky_stream));
+     CUCHK(cudaStreamSynchronize(e->stream));
+     TRY(e->plan_sky.alloc(std::max<size_t>(e->plan_sky.bytes, hs.size() * sizeof(SkyParam))));
+     TRY(e->plan_tp.alloc(std::max<size_t>(e->plan_tp.bytes, ht.size() * sizeof(TmplParam))));
+     CUCHK(cudaMemcpy(e->plan_sky.p, hs.data(), hs.size() * sizeof(SkyParam), cudaMemcpyHostToDevice));
+     CUCHK(cudaMemcpy(e->plan_tp.p, ht.data(), ht.size() * sizeof(TmplParam), cudaMemcpyHostToDevice));
+     e->sparse_now = e->sparse_f && e->form == TDF_FORM_SPLIT && !(e->opts.blocks_avg && e->nblk_mu > 0);
+     for (int pass = 0; pass < 2; pass++) {
+          uint64_t key = 1469598103934665603ull;
+          for (const PlanBatch &B : pb) {
+               const uint64_t f[] = {(uint64_t)B.slot, (uint64_t)B.nb, (uint64_t)B.nt, (uint64_t)B.sky_off,
+                                     (uint64_t)B.tp_off};
+               key = fnv1a(key, f, sizeof(f));
+          }
+          const uintptr_t cfg[] = {(uintptr_t)e->Tc, (uintptr_t)e->Gt, (uintptr_t)e->nlanes, (uintptr_t)e->sparse_now,
+                                   (uintptr_t)e->plan_sky.p, (uintptr_t)e->plan_tp.p, (uintptr_t)e->trig[0].p,
+                                   (uintptr_t)e->trig[1].p, (uintptr_t)e->trig_cap};
+          key = fnv1a(key, cfg, sizeof(cfg));
+          TRY(run_plan(e, pb, key));
+          CUCHK(cudaStreamSynchronize(e->stream));
+          const unsigned errf = (unsigned)((e->h_cnt[1] | e->h_cnt[3]) & 0xffffffffu);
+          if (errf & ERR_OVERFLOW)
+               return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
+          if (errf & ERR_STAGE_TIMEOUT)
+               return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
+          if ((errf & ERR_NEED_FULL_F) && e->sparse_now) {
+               e->sparse_now = false;   // once more with the full F store
+               continue;
+          }
+          if (errf & ERR_NEED_FULL_F) return set_error(TDF_ERR_CUDA, "trigger selection asked for the full F store twice");
+          *ntrig = (int64_t)(e->h_cnt[0] + e->h_cnt[2]);
+          return TDF_OK;
+     }
+     return set_error(TDF_ERR_CUDA, "plan did not complete");
+}
+
 // add_signal (init.c:365-504) on the resident xDat.  The constants are
 // formed here as the reference forms them; k_signal computes s_n[i] into the
 // sky-stage scratch B0 (idle between searches), k_add_signal adds h0 s_n[i].
@@ -1645,7 +1963,7 @@ int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0_out, 
      if (in_band) *in_band = 0;
      CUCHK(cudaSetDevice(e->dev));
      const int N = e->N, nifo = e->nifo;
-     const double dt = e->seg.dt;
+     const double dt = e->S().seg.dt;
      const int dseg = sig->seg - sig->reffr;
      double freqo0 = 2 * M_PI * sig->freq * dt;
      const double freqo1 = M_PI * sig->fdot * dt * dt;
@@ -1677,8 +1995,8 @@ int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0_out, 
      cudaStream_t st = e->stream;
      double *s = e->B0.as<double>();
      double *part = e->partial.as<double>();
-     k_signal<<<dim3(nblk, nifo), 256, 0, st>>>(e->xdat.as<float>(), e->detssb.as<double>(), e->cosm.as<double>(),
-                                                e->sinm.as<double>(), e->detp.as<DetParam>(), N, e->Nal, P, s, part);
+     k_signal<<<dim3(nblk, nifo), 256, 0, st>>>(e->S().xdat.as<float>(), e->S().detssb.as<double>(), e->S().cosm.as<double>(),
+                                                e->S().sinm.as<double>(), e->S().detp.as<DetParam>(), N, e->Nal, P, s, part);
      CUCHK(cudaGetLastError());
      double h0 = sig->h0;
      if (sig->snr > 0.) {
@@ -1689,12 +2007,12 @@ int tdf_engine_add_signal(tdf_engine *e, const tdf_signal *sig, double *h0_out, 
           for (int n = 0; n < nifo; n++) {
                double sum = 0.;
                for (int b = 0; b < nblk; b++) sum += ps[(size_t)n * nblk + b];
-               net += sum / e->dets[n].sig2;
+               net += sum / e->S().dets[n].sig2;
           }
           if (!(net > 0.)) return set_error(TDF_ERR_INVALID, "signal has no power in the data (snr form)");
           h0 = sig->snr / std::sqrt(net);
      }
-     k_add_signal<<<dim3(nblk, nifo), 256, 0, st>>>(e->xdat.as<float>(), s, N, e->Nal, h0);
+     k_add_signal<<<dim3(nblk, nifo), 256, 0, st>>>(e->S().xdat.as<float>(), s, N, e->Nal, h0);
      CUCHK(cudaGetLastError());
      CUCHK(cudaStreamSynchronize(st));
      e->launches += 2;
@@ -1724,7 +2042,7 @@ int tdf_engine_get_xdat(tdf_engine *e, int32_t det, float *xdat, int64_t n) {
           return set_error(TDF_ERR_INVALID, "detector %d of %d, %lld samples of %d", det, e->nifo, (long long)n, e->N);
      CUCHK(cudaSetDevice(e->dev));
      CUCHK(cudaStreamSynchronize(e->stream));
-     CUCHK(cudaMemcpy(xdat, e->xdat.as<float>() + (size_t)det * e->Nal, n * sizeof(float), cudaMemcpyDeviceToHost));
+     CUCHK(cudaMemcpy(xdat, e->S().xdat.as<float>() + (size_t)det * e->Nal, n * sizeof(float), cudaMemcpyDeviceToHost));
      return TDF_OK;
 }
 
@@ -1753,7 +2071,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[0], 0));
      CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[0], sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
      CUCHK(cudaMemsetAsync(e->counters[0].p, 0, 2 * sizeof(unsigned long long), e->stream));
-     for (int l = 0; l < e->nlanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+     for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
      e->sparse_now = false;   // the spectrum itself is the output: the full F store
      TRY(run_templates(e, e->tparam.as<TmplParam>(), 1));
      CUCHK(cudaMemcpyAsync(e->h_cnt, e->counters[0].p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
@@ -1796,51 +2114,94 @@ int tdf_engine_set_stream(tdf_engine *e, void *stream) {
      return TDF_OK;
 }
 
+// Times device-only searches of the caller's points (the fastest of plain
+// launches, capture and replay when graphs are on) for one setting.
+static int autotune_time(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn, cudaEvent_t a,
+                         cudaEvent_t b, float *best_ms) {
+     std::vector<HostPoint> pts;
+     std::vector<HostTmpl> tm;
+     int64_t ntrig = 0;
+     float m2 = 1e30f;
+     const int reps = e->use_graphs ? 3 : 2;
+     for (int rep = 0; rep < reps; rep++) {
+          CUCHK(cudaEventRecord(a, e->stream));
+          TRY(search_core(e, npts, pm, mm, nn, nullptr, pts, tm, false, &ntrig));
+          CUCHK(cudaEventRecord(b, e->stream));
+          CUCHK(cudaEventSynchronize(b));
+          float ms = 0.f;
+          CUCHK(cudaEventElapsedTime(&ms, a, b));
+          m2 = std::min(m2, ms);
+     }
+     *best_ms = m2;
+     return TDF_OK;
+}
+
+// Coordinate search: the templates per chunk (6..48) at the current lanes and
+// group size, then the lanes (2..4) at the best chunk size, then the
+// templates per resolve group (32, 64, 128).
 int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
                         int32_t *best) {
      if (!e) return set_error(TDF_ERR_INVALID, "null engine");
      CUCHK(cudaSetDevice(e->dev));
-     static const int cands[] = {6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 37, 41, 48};
+     static const int tcs[] = {6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 37, 41, 48};
+     static const int lanes[] = {2, 3, 4};
+     static const int gts[] = {32, 64, 128};
      cudaEvent_t a, b;
      CUCHK(cudaEventCreate(&a));
      CUCHK(cudaEventCreate(&b));
-     const int keep = e->Tc;
-     double best_ms = 1e300;
-     int best_tc = keep;
-     std::vector<HostPoint> pts;
-     std::vector<HostTmpl> tm;
-     int64_t ntrig = 0;
+     const int keep_tc = e->Tc, keep_l = e->nlanes, keep_g = e->Gt;
      int st = TDF_OK;
-     for (int c : cands) {
-          if (c > e->TcMax) continue;
+     float best_ms = 1e30f, ms = 0.f;
+     int btc = keep_tc, bl = keep_l, bg = keep_g;
+     for (int c : tcs) {
+          if (c > e->TcMax || st != TDF_OK) continue;
           e->Tc = c;
-          float ms = 0.f, m2 = 1e30f;
-          // with graphs: plain launches, capture, replay (a replay is what a search runs)
-          const int reps = e->use_graphs ? 3 : 2;
-          for (int rep = 0; rep < reps && st == TDF_OK; rep++) {
-               cudaEventRecord(a, e->stream);
-               st = search_core(e, npts, pm, mm, nn, nullptr, pts, tm, false, &ntrig);
-               cudaEventRecord(b, e->stream);
-               cudaEventSynchronize(b);
-               cudaEventElapsedTime(&ms, a, b);
-               m2 = std::min(m2, ms);
-          }
-          if (st != TDF_OK) break;
-          if (m2 < best_ms) {
-               best_ms = m2;
-               best_tc = c;
+          st = autotune_time(e, npts, pm, mm, nn, a, b, &ms);
+          if (st == TDF_OK && ms < best_ms) {
+               best_ms = ms;
+               btc = c;
           }
      }
+     e->Tc = btc;
+     for (int l : lanes) {
+          if (st != TDF_OK || l == bl) continue;
+          e->nlanes = l;
+          st = autotune_time(e, npts, pm, mm, nn, a, b, &ms);
+          if (st == TDF_OK && ms < best_ms) {
+               best_ms = ms;
+               bl = l;
+          }
+     }
+     e->nlanes = bl;
+     for (int g : gts) {
+          if (st != TDF_OK || g == bg) continue;
+          e->Gt = g;
+          st = autotune_time(e, npts, pm, mm, nn, a, b, &ms);
+          if (st == TDF_OK && ms < best_ms) {
+               best_ms = ms;
+               bg = g;
+          }
+     }
+     e->Gt = bg;
      cudaEventDestroy(a);
      cudaEventDestroy(b);
      if (st != TDF_OK) {
-          e->Tc = keep;
+          e->Tc = keep_tc;
+          e->nlanes = keep_l;
+          e->Gt = keep_g;
           return st;
      }
-     e->Tc = best_tc;
      graphs_clear(e);   // the candidates' graphs
      autotune_cache_store(e);
-     if (best) *best = best_tc;
+     if (best) *best = btc;
+     return TDF_OK;
+}
+
+int tdf_engine_get_tuning(tdf_engine *e, int32_t *templates_per_chunk, int32_t *lanes, int32_t *group_templates) {
+     if (!e) return set_error(TDF_ERR_INVALID, "null engine");
+     if (templates_per_chunk) *templates_per_chunk = e->Tc;
+     if (lanes) *lanes = e->nlanes;
+     if (group_templates) *group_templates = e->Gt;
      return TDF_OK;
 }
 

@@ -167,6 +167,31 @@ class Engine:
         _check(self.lib, st)
         return nrec.value, ntrig.value
 
+    def add_segment(self, segment: _abi.TdfSegment) -> int:
+        """Uploads another segment of the engine's sizes; returns its slot."""
+        slot = C.c_int32(0)
+        _check(self.lib, self.lib.tdf_engine_add_segment(self.h, C.byref(segment), C.byref(slot)))
+        return slot.value
+
+    def upload_segment(self, slot: int, segment: _abi.TdfSegment):
+        _check(self.lib, self.lib.tdf_engine_upload_segment(self.h, int(slot), C.byref(segment)))
+
+    def search_segments_device(self, slots, npts, pm, mm, nn) -> Tuple[int, int]:
+        """Device-only pass over several resident segments (slot k searches
+        npts[k] of the points, in order); returns (records, triggers)."""
+        slots = np.ascontiguousarray(slots, dtype=np.int32)
+        npts = np.ascontiguousarray(npts, dtype=np.int32)
+        pm = np.ascontiguousarray(pm, dtype=np.int32)
+        mm = np.ascontiguousarray(mm, dtype=np.float32)
+        nn = np.ascontiguousarray(nn, dtype=np.float32)
+        assert int(npts.sum()) == len(pm) == len(mm) == len(nn)
+        nrec, ntrig = C.c_int64(0), C.c_int64(0)
+        st = self.lib.tdf_search_segments_device(self.h, len(slots), _p(slots, C.c_int32), _p(npts, C.c_int32),
+                                                 _p(pm, C.c_int32), _p(mm, C.c_float), _p(nn, C.c_float),
+                                                 C.byref(nrec), C.byref(ntrig))
+        _check(self.lib, st)
+        return nrec.value, ntrig.value
+
     def fstat(self, pm: int, mm: float, nn: float, ss: float) -> np.ndarray:
         F = np.zeros(self.nF, dtype=np.float64)
         st = self.lib.tdf_fstat_spectrum(self.h, int(pm), float(mm), float(nn), float(ss), _p(F, C.c_double), len(F))
@@ -220,6 +245,13 @@ class Engine:
         _check(self.lib, self.lib.tdf_engine_autotune(self.h, len(pm), _p(pm, C.c_int32), _p(mm, C.c_float),
                                                       _p(nn, C.c_float), C.byref(best)))
         return best.value
+
+    def tuning(self) -> dict:
+        """The launch configuration in use: templates per chunk, lanes,
+        templates per resolve group."""
+        tc, ln, gt = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        _check(self.lib, self.lib.tdf_engine_get_tuning(self.h, C.byref(tc), C.byref(ln), C.byref(gt)))
+        return {"templates_per_chunk": tc.value, "lanes": ln.value, "group_templates": gt.value}
 
     @property
     def templates_per_chunk(self) -> int:

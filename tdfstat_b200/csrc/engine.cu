@@ -383,7 +383,8 @@ struct tdf_engine {
      // whole-call plans (tdf_search_segments_device): every batch's sky and
      // template parameters on the device at once, the call's work captured
      // as one graph, keyed by a hash of its batch list and configuration
-     DevBuf plan_sky, plan_tp;
+     DevBuf plan_sky, plan_tp, plan_pts;
+     int plan_npts = 0;
      cudaEvent_t plan_ev = nullptr;
      struct PlanGraph {
           uint64_t key = 0;
@@ -695,7 +696,7 @@ static void graphs_clear(tdf_engine *e) {
 static void engine_free(tdf_engine *e) {
      graphs_clear(e);
      for (SegData &d : e->sdv) d.release();
-     DevBuf *bufs[] = {&e->pco, &e->gco, &e->plan_sky, &e->plan_tp, &e->skyp[0],
+     DevBuf *bufs[] = {&e->pco, &e->gco, &e->plan_sky, &e->plan_tp, &e->plan_pts, &e->skyp[0],
                        &e->skyp[1], &e->B0, &e->B1, &e->B2, &e->shftf, &e->partial, &e->aabb[0], &e->aabb[1],
                        &e->xab[0], &e->xab[1], &e->s2[0], &e->s2[1], &e->xa64[0], &e->xa64[1], &e->xb64[0],
                        &e->xb64[1], &e->t1[0], &e->t1[1], &e->tparam, &e->trig[0], &e->trig[1],
@@ -1432,6 +1433,42 @@ struct PlanBatch {
      size_t sky_off, tp_off;
 };
 
+// One sky point of a plan: what tmpl_setup() needs to form its templates
+// (the segment's grid-matrix entries travel with it, segments differ).
+struct PlanPoint {
+     double het0, M0, M4, M5, M9, M13;
+     float mm, nn, smin, sstep;
+     int32_t iss, slot;     // spindowns; the point's index in its sky batch
+     uint32_t id0, tp0;     // template number and plan index of its first spindown
+};
+
+// tmpl_setup() on the device, one CTA per point: the same IEEE operations in
+// the same order (no contraction), so the parameters equal the host's bit
+// for bit.  grid (points), 128 threads
+__global__ void __launch_bounds__(128) k_plan_templates(const PlanPoint *__restrict__ pts, TmplParam *__restrict__ tp,
+                                                        int split)
+{
+     const PlanPoint P = pts[blockIdx.x];
+     for (int s = threadIdx.x; s < P.iss; s += blockDim.x) {
+          const float ss = __fadd_rn(P.smin, __fmul_rn((float)s, P.sstep));
+          TmplParam q;
+          q.spnd = __dadd_rn(__dadd_rn(__dmul_rn((double)ss, P.M5), __dmul_rn((double)P.nn, P.M9)),
+                             __dmul_rn((double)P.mm, P.M13));
+          const double r = fmod(__dmul_rn((double)ss, P.M4), P.M0);
+          q.het1 = r < 0 ? __dadd_rn(r, P.M0) : r;
+          if (split) {
+               float h1 = (float)r;
+               if (h1 < 0) h1 = (float)__dadd_rn((double)h1, P.M0);
+               q.sgnl0 = (double)(float)__dadd_rn(P.het0, (double)h1);
+          } else {
+               q.sgnl0 = __dadd_rn(P.het0, q.het1);
+          }
+          q.slot = P.slot;
+          q.id = P.id0 + (uint32_t)s;
+          tp[P.tp0 + s] = q;
+     }
+}
+
 static uint64_t fnv1a(uint64_t h, const void *p, size_t n) {
      const unsigned char *c = (const unsigned char *)p;
      for (size_t i = 0; i < n; i++) {
@@ -1444,6 +1481,10 @@ static uint64_t fnv1a(uint64_t h, const void *p, size_t n) {
 static int enqueue_plan(tdf_engine *e, const std::vector<PlanBatch> &pb) {
      const SkyParam *dsky = e->plan_sky.as<SkyParam>();
      const TmplParam *dtp = e->plan_tp.as<TmplParam>();
+     k_plan_templates<<<e->plan_npts, 128, 0, e->stream>>>(e->plan_pts.as<PlanPoint>(), e->plan_tp.as<TmplParam>(),
+                                                            e->form == TDF_FORM_SPLIT);
+     CUCHK(cudaGetLastError());
+     e->launches++;
      for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
      for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
      // the sky stream's first work of the plan follows this point of the engine stream
@@ -1513,6 +1554,34 @@ static int run_plan(tdf_engine *e, const std::vector<PlanBatch> &pb, uint64_t ke
      }
      CUCHK(cudaGraphLaunch(g.exec, e->stream));
      e->launches += g.launches;
+     return TDF_OK;
+}
+
+// TDF_CHECK_PLAN=1: the templates the device formed for a plan, compared bit
+// for bit with tmpl_setup() on the host for the same points (a self-check of
+// k_plan_templates; the search's own path never reads them back).  seg[i]
+// is the segment slot of plan point i.
+static int plan_check(tdf_engine *e, const std::vector<PlanPoint> &hp, const std::vector<int> &seg, int64_t ntm) {
+     std::vector<TmplParam> dev((size_t)ntm);
+     CUCHK(cudaMemcpy(dev.data(), e->plan_tp.p, (size_t)ntm * sizeof(TmplParam), cudaMemcpyDeviceToHost));
+     for (size_t i = 0; i < hp.size(); i++) {
+          const PlanPoint &P = hp[i];
+          HostPoint H;
+          H.sp.het0 = P.het0;
+          e->act = seg[i];
+          for (int s2 = 0; s2 < P.iss; s2++) {
+               HostTmpl T;
+               tmpl_setup(e, H, P.mm, P.nn, P.smin + s2 * P.sstep, T);
+               const TmplParam &d = dev[P.tp0 + s2];
+               if (memcmp(&d.spnd, &T.spnd, 8) || memcmp(&d.het1, &T.het1, 8) || memcmp(&d.sgnl0, &T.sgnl0, 8) ||
+                   d.slot != P.slot || d.id != P.id0 + (uint32_t)s2) {
+                    e->act = 0;
+                    return set_error(TDF_ERR_CUDA, "plan self-check: template %d of plan point %zu differs from "
+                                     "the host's", s2, i);
+               }
+          }
+     }
+     e->act = 0;
      return TDF_OK;
 }
 
@@ -1870,7 +1939,8 @@ int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots
      // the sky and template parameters as search_core forms them
      std::vector<PlanBatch> pb;
      std::vector<SkyParam> hs;
-     std::vector<TmplParam> ht;
+     std::vector<PlanPoint> hp;
+     std::vector<int> hp_seg;   // segment slot of each plan point
      int64_t ntm = 0;
      size_t off = 0;
      for (int k = 0; k < nseg; k++) {
@@ -1891,23 +1961,31 @@ int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots
                B.slot = slots[k];
                B.nb = (int)std::min<size_t>(e->Bs, inside.size() - b0);
                B.sky_off = hs.size();
-               B.tp_off = ht.size();
+               B.tp_off = (size_t)ntm;
                B.nt = 0;
+               const double *M = e->S().seg.M;
                for (int j = 0; j < B.nb; j++) {
                     const int ip = inside[b0 + j];
                     const HostPoint &P = pts[ip];
                     hs.push_back(P.sp);
-                    for (int s2 = 0; s2 < P.iss_size; s2++) {
-                         HostTmpl T;
-                         tmpl_setup(e, P, mm[off + ip], nn[off + ip], P.smin + s2 * e->opts.sstep, T);
-                         TmplParam q;
-                         q.het1 = T.het1;
-                         q.spnd = T.spnd;
-                         q.sgnl0 = T.sgnl0;
-                         q.slot = j;
-                         q.id = (uint32_t)(ntm++);
-                         ht.push_back(q);
-                    }
+                    PlanPoint q;
+                    q.het0 = P.sp.het0;
+                    q.M0 = M[0];
+                    q.M4 = M[4];
+                    q.M5 = M[5];
+                    q.M9 = M[9];
+                    q.M13 = M[13];
+                    q.mm = mm[off + ip];
+                    q.nn = nn[off + ip];
+                    q.smin = P.smin;
+                    q.sstep = e->opts.sstep;
+                    q.iss = P.iss_size;
+                    q.slot = j;
+                    q.id0 = (uint32_t)ntm;
+                    q.tp0 = (uint32_t)ntm;
+                    hp.push_back(q);
+                    hp_seg.push_back(slots[k]);
+                    ntm += P.iss_size;
                     B.nt += P.iss_size;
                }
                pb.push_back(B);
@@ -1922,10 +2000,14 @@ int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots
      CUCHK(cudaStreamSynchronize(e->sky_stream));
      CUCHK(cudaStreamSynchronize(e->stream));
      TRY(e->plan_sky.alloc(std::max<size_t>(e->plan_sky.bytes, hs.size() * sizeof(SkyParam))));
-     TRY(e->plan_tp.alloc(std::max<size_t>(e->plan_tp.bytes, ht.size() * sizeof(TmplParam))));
+     TRY(e->plan_pts.alloc(std::max<size_t>(e->plan_pts.bytes, hp.size() * sizeof(PlanPoint))));
+     TRY(e->plan_tp.alloc(std::max<size_t>(e->plan_tp.bytes, (size_t)ntm * sizeof(TmplParam))));
      CUCHK(cudaMemcpy(e->plan_sky.p, hs.data(), hs.size() * sizeof(SkyParam), cudaMemcpyHostToDevice));
-     CUCHK(cudaMemcpy(e->plan_tp.p, ht.data(), ht.size() * sizeof(TmplParam), cudaMemcpyHostToDevice));
+     CUCHK(cudaMemcpy(e->plan_pts.p, hp.data(), hp.size() * sizeof(PlanPoint), cudaMemcpyHostToDevice));
+     e->plan_npts = (int)hp.size();
      e->sparse_now = e->sparse_f && e->form == TDF_FORM_SPLIT && !(e->opts.blocks_avg && e->nblk_mu > 0);
+     const char *cp = getenv("TDF_CHECK_PLAN");
+     const bool check_plan = cp && cp[0] == '1';
      for (int pass = 0; pass < 2; pass++) {
           uint64_t key = 1469598103934665603ull;
           for (const PlanBatch &B : pb) {
@@ -1934,11 +2016,13 @@ int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots
                key = fnv1a(key, f, sizeof(f));
           }
           const uintptr_t cfg[] = {(uintptr_t)e->Tc, (uintptr_t)e->Gt, (uintptr_t)e->nlanes, (uintptr_t)e->sparse_now,
-                                   (uintptr_t)e->plan_sky.p, (uintptr_t)e->plan_tp.p, (uintptr_t)e->trig[0].p,
+                                   (uintptr_t)e->plan_sky.p, (uintptr_t)e->plan_tp.p, (uintptr_t)e->plan_pts.p,
+                                   (uintptr_t)e->plan_npts, (uintptr_t)e->trig[0].p,
                                    (uintptr_t)e->trig[1].p, (uintptr_t)e->trig_cap};
           key = fnv1a(key, cfg, sizeof(cfg));
           TRY(run_plan(e, pb, key));
           CUCHK(cudaStreamSynchronize(e->stream));
+          if (check_plan) TRY(plan_check(e, hp, hp_seg, ntm));
           const unsigned errf = (unsigned)((e->h_cnt[1] | e->h_cnt[3]) & 0xffffffffu);
           if (errf & ERR_OVERFLOW)
                return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);

@@ -7,7 +7,8 @@ seeds and segment numbers: other noise, gaps, grid matrix and injection
 phase) searched in one call must give the record and trigger counts of
 separate single-segment engines with the same options, in every order of
 the slots, on the first (plain launches), second (capture) and third
-(replay) call, in both forms.
+(replay) call, in both forms; the template parameters the call forms on
+the device must equal the host's bit for bit.
 """
 import dataclasses
 import shutil
@@ -37,8 +38,11 @@ def three_jobs():
 
 
 @pytest.mark.parametrize("form", ["split", "fp64"])
-def test_segments_in_one_call_match_separate_engines(three_jobs, form):
+def test_segments_in_one_call_match_separate_engines(three_jobs, monkeypatch, form):
+    """TDF_CHECK_PLAN=1 also compares the template parameters the device forms
+    for the call with the host's (bit for bit) on every call."""
     from tdfstat_b200.engine import Engine
+    monkeypatch.setenv("TDF_CHECK_PLAN", "1")
     jobs = three_jobs[form]
     opts = jobs[0].search_opts()
     pts = [j.sky_points() for j in jobs]

@@ -101,6 +101,24 @@ static int set_smem(K kern, size_t smem) {
      return TDF_OK;
 }
 
+// Kernels of the sky stage (the FP64 interpolation passes run with one
+// array, NA = 1; the spindown passes with two).  A captured graph holding
+// both gets the sky stage's kernel nodes at the low stream priority and the
+// others at the high one, as the two streams have them when launched
+// directly (set_graph_priorities).
+static std::mutex g_sky_mu;
+static std::vector<const void *> g_sky_kernels;
+
+static void register_sky_kernel(const void *k) {
+     std::lock_guard<std::mutex> lk(g_sky_mu);
+     if (std::find(g_sky_kernels.begin(), g_sky_kernels.end(), k) == g_sky_kernels.end()) g_sky_kernels.push_back(k);
+}
+
+static bool is_sky_kernel(const void *k) {
+     std::lock_guard<std::mutex> lk(g_sky_mu);
+     return std::find(g_sky_kernels.begin(), g_sky_kernels.end(), k) != g_sky_kernels.end();
+}
+
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
 static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T> *tw, cudaStream_t st) {
      size_t smem = pass_smem_bytes<T, L, NA>();
@@ -113,6 +131,7 @@ static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T
           smem += Epi::template table_bytes<L>(epi.N2);
      }
      auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi>;
+     if constexpr (NA == 1) register_sky_kernel((const void *)kern);
      TRY(set_smem(kern, smem));
      kern<<<grid, pass_threads<L>(), smem, st>>>(pro, epi, tw);
      CUCHK(cudaGetLastError());
@@ -130,6 +149,7 @@ static int launch_row_L(dim3 grid, const Src &src_in, const Epi &epi, const cx<T
           smem += 16;
      }
      auto kern = k_rowpass<T, L, SIGN, NA, Src, Epi>;
+     if constexpr (NA == 1) register_sky_kernel((const void *)kern);
      TRY(set_smem(kern, smem));
      kern<<<grid, pass_threads<L>(), smem, st>>>(src, epi, tw);
      CUCHK(cudaGetLastError());
@@ -1123,6 +1143,37 @@ static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
      return TDF_OK;
 }
 
+static int set_graph_priorities(const tdf_engine *e, cudaGraph_t g) {
+     if (!e->overlap || !e->stream_outranks_sky) return TDF_OK;
+     {
+          // the sky kernels launched with <<<>>> (the passes register themselves)
+          static std::once_flag once;
+          std::call_once(once, [] {
+               register_sky_kernel((const void *)k_sky_prep);
+               register_sky_kernel((const void *)k_sky_sums);
+               register_sky_kernel((const void *)k_spline_fwd);
+               register_sky_kernel((const void *)k_spline_bwd);
+               register_sky_kernel((const void *)k_splint);
+          });
+     }
+     size_t n = 0;
+     CUCHK(cudaGraphGetNodes(g, nullptr, &n));
+     std::vector<cudaGraphNode_t> nodes(n);
+     CUCHK(cudaGraphGetNodes(g, nodes.data(), &n));
+     for (cudaGraphNode_t nd : nodes) {
+          cudaGraphNodeType ty;
+          CUCHK(cudaGraphNodeGetType(nd, &ty));
+          if (ty != cudaGraphNodeTypeKernel) continue;
+          cudaKernelNodeParams kp;
+          CUCHK(cudaGraphKernelNodeGetParams(nd, &kp));
+          cudaKernelNodeAttrValue v;
+          memset(&v, 0, sizeof(v));
+          v.priority = is_sky_kernel(kp.func) ? e->prio_low : e->prio_high;
+          CUCHK(cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributePriority, &v));
+     }
+     return TDF_OK;
+}
+
 // The spindown stage of the current batch (nt templates uploaded to tparam):
 // the first time a configuration is seen its kernels are launched one by one;
 // the second time they are captured (all lanes) into a graph, which later
@@ -1165,6 +1216,12 @@ static int run_templates_batch(tdf_engine *e, int nt) {
                if (graph) cudaGraphDestroy(graph);
                e->launches = l0;
                return st != TDF_OK ? st : set_error(TDF_ERR_CUDA, "stream capture: %s", cudaGetErrorString(ce));
+          }
+          const int ps = set_graph_priorities(e, graph);
+          if (ps != TDF_OK) {
+               cudaGraphDestroy(graph);
+               e->launches = l0;
+               return ps;
           }
           const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
           cudaGraphDestroy(graph);
@@ -1541,6 +1598,12 @@ static int run_plan(tdf_engine *e, const std::vector<PlanBatch> &pb, uint64_t ke
                if (graph) cudaGraphDestroy(graph);
                e->launches = l0;
                return st != TDF_OK ? st : set_error(TDF_ERR_CUDA, "stream capture: %s", cudaGetErrorString(ce));
+          }
+          const int ps = set_graph_priorities(e, graph);
+          if (ps != TDF_OK) {
+               cudaGraphDestroy(graph);
+               e->launches = l0;
+               return ps;
           }
           const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
           cudaGraphDestroy(graph);

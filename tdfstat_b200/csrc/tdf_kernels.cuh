@@ -509,12 +509,17 @@ struct DemodSplitILT {
                     const float4 *x = xp + m * de;
                     const float *s = sp + m * de;
                     if (nf == 2) {
+                         // both detectors' rotated operands summed in one
+                         // chain of fused multiply-adds per component
                          const float2 ss = __ldg(reinterpret_cast<const float2 *>(s));
-                         DemodSplit::rot(__ldg(x), fmaf(spf, ss.x, pr), fa, fb);
-                         float2 pa, pb;
-                         DemodSplit::rot(__ldg(x + 1), fmaf(spf, ss.y, pr), pa, pb);
-                         fa = cadd(fa, pa);
-                         fb = cadd(fb, pb);
+                         const float4 x0 = __ldg(x), x1 = __ldg(x + 1);
+                         float s0, c0, s1, c1;
+                         __sincosf(fmaf(spf, ss.x, pr), &s0, &c0);
+                         __sincosf(fmaf(spf, ss.y, pr), &s1, &c1);
+                         fa.x = fmaf(x0.x, c0, fmaf(x0.y, s0, fmaf(x1.x, c1, x1.y * s1)));
+                         fa.y = fmaf(x0.y, c0, fmaf(-x0.x, s0, fmaf(x1.y, c1, -x1.x * s1)));
+                         fb.x = fmaf(x0.z, c0, fmaf(x0.w, s0, fmaf(x1.z, c1, x1.w * s1)));
+                         fb.y = fmaf(x0.w, c0, fmaf(-x0.z, s0, fmaf(x1.w, c1, -x1.z * s1)));
                     } else if (nf == 1) {
                          DemodSplit::rot(__ldg(x), fmaf(spf, __ldg(s), pr), fa, fb);
                     } else {

@@ -416,6 +416,7 @@ struct tdf_engine {
      std::vector<PlanGraph> plan_graphs;
      uint64_t graph_tick = 0;
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
+     bool graph_prio = true;   // TDF_GRAPH_PRIORITY=0 leaves captured kernel nodes at their default priority
      bool row_bulk = true;     // row passes fetch their rows by bulk copies (TDF_ROW_BULK=0: per thread)
      // split form: the row pass keeps F on the chip and hands over only the
      // candidates and the edge bins of its runs (TDF_FULL_F=1: full F ring);
@@ -1144,7 +1145,7 @@ static int run_templates(tdf_engine *e, const TmplParam *dtp, int nt) {
 }
 
 static int set_graph_priorities(const tdf_engine *e, cudaGraph_t g) {
-     if (!e->overlap || !e->stream_outranks_sky) return TDF_OK;
+     if (!e->overlap || !e->stream_outranks_sky || !e->graph_prio) return TDF_OK;
      {
           // the sky kernels launched with <<<>>> (the passes register themselves)
           static std::once_flag once;
@@ -1750,6 +1751,8 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
      const char *gr = getenv("TDF_GRAPHS");
      if (gr && gr[0] == '0') e->use_graphs = false;
+     const char *gp = getenv("TDF_GRAPH_PRIORITY");
+     if (gp && gp[0] == '0') e->graph_prio = false;
      const char *ff = getenv("TDF_FULL_F");
      if (ff && ff[0] == '1') e->sparse_f = false;
      const char *rb = getenv("TDF_ROW_BULK");

@@ -117,17 +117,6 @@ template <typename T, int L> struct LineGeom {
 
 constexpr int LINES = 8;   // lines (columns or rows) per CTA
 
-// Two FP32 arrays transformed together (the spindown stage's Fa, Fb) share
-// one line buffer: element p of both arrays is one 16-byte word
-// (a.re, a.im, b.re, b.im) at pad(p), so each Stockham exchange is one
-// 128-bit access per element instead of two 64-bit ones.  Lines are STRIDE
-// 16-byte words apart, STRIDE odd: the 8 lanes of a quarter-warp (8 lines,
-// one t) fall on distinct bank groups.
-template <int L> struct LineGeom2 {
-     static constexpr int LP = L + L / 8;
-     static constexpr int STRIDE = LP + (LP % 2 == 0 ? 1 : 0);
-};
-
 // Apply the Stockham twiddles of a pass (radix R, span NS) to the butterflies
 // a thread owns, for all NA lines it holds (the twiddles depend only on the
 // butterfly, so they are formed once).  tw[m] = e^{-2 pi i m / L}, m < L
@@ -212,75 +201,6 @@ __device__ __forceinline__ void pass_load(cx<T> (&v)[8], const cx<T> *s, int t) 
           const cx<T> *d = s + pad8(t + q * (L / 8));
 #pragma unroll
           for (int r = 0; r < R; r++) v[q + r * (8 / R)] = d[r * ((L / R) + (L / R) / 8)];
-     }
-}
-
-// pass_store / pass_load for the interleaved two-array line buffer
-template <int L, int R>
-__device__ __forceinline__ void pass_store2(const float2 (&v)[2][8], float4 *s, int t, int NS) {
-#pragma unroll
-     for (int q = 0; q < 8 / R; q++) {
-          const int j = t + q * (L / 8);
-          if (NS == 1 && R == 8) {
-               float4 *d = s + 9 * j;
-#pragma unroll
-               for (int r = 0; r < R; r++) {
-                    const int i = q + r * (8 / R);
-                    d[r] = make_float4(v[0][i].x, v[0][i].y, v[1][i].x, v[1][i].y);
-               }
-          } else {
-               static_assert(R == 8, "stores come from radix-8 passes");
-               float4 *d = s + pad8((j / NS) * NS * R + (j % NS));
-#pragma unroll
-               for (int r = 0; r < R; r++) {
-                    const int i = q + r * (8 / R);
-                    d[r * (NS + NS / 8)] = make_float4(v[0][i].x, v[0][i].y, v[1][i].x, v[1][i].y);
-               }
-          }
-     }
-}
-
-template <int L, int R>
-__device__ __forceinline__ void pass_load2(float2 (&v)[2][8], const float4 *s, int t) {
-     static_assert((L / R) % 8 == 0, "line length per radix must be a multiple of 8");
-#pragma unroll
-     for (int q = 0; q < 8 / R; q++) {
-          const float4 *d = s + pad8(t + q * (L / 8));
-#pragma unroll
-          for (int r = 0; r < R; r++) {
-               const float4 w = d[r * ((L / R) + (L / R) / 8)];
-               v[0][q + r * (8 / R)] = make_float2(w.x, w.y);
-               v[1][q + r * (8 / R)] = make_float2(w.z, w.w);
-          }
-     }
-}
-
-// line_fft for two FP32 arrays in one interleaved line buffer s (LineGeom2);
-// the same passes, twiddles and butterflies in the same order.
-template <int L, int SIGN>
-__device__ __forceinline__ void line_fft2(float2 (&v)[2][8], float4 *s, const float2 *tw, int t) {
-     using G = LineGeom<float, L>;
-     int NS = 1;
-#pragma unroll
-     for (int p = 0; p < G::P8; p++) {
-          if (p > 0) pass_twiddle<float, L, 8, SIGN, 2>(v, tw, t, NS);
-          pass_dft<8, SIGN>(v[0]);
-          pass_dft<8, SIGN>(v[1]);
-          const bool last = (p == G::P8 - 1) && (G::RL == 1);
-          if (!last) {
-               pass_store2<L, 8>(v, s, t, NS);
-               __syncthreads();
-               if (p + 1 < G::P8) pass_load2<L, 8>(v, s, t);
-               else pass_load2<L, (G::RL > 1 ? G::RL : 8)>(v, s, t);
-               __syncthreads();
-          }
-          NS *= 8;
-     }
-     if (G::RL > 1) {
-          constexpr int RR = G::RL > 1 ? G::RL : 2;
-          pass_twiddle<float, L, RR, SIGN, 2>(v, tw, t, NS);
-          pass_dft<RR, SIGN>(v[0]);
-          pass_dft<RR, SIGN>(v[1]);
      }
 }
 

@@ -470,6 +470,20 @@ struct DemodSplit {
      }
 };
 
+// Two detectors' demodulated operands summed in one chain of fused
+// multiply-adds per component: fa + i... = x0 (c0 - i s0) + x1 (c1 - i s1)
+// for the two arrays of x = (a.re, a.im, b.re, b.im).
+__device__ __forceinline__ void demod2(const float4 x0, const float4 x1, float ph0, float ph1, float2 &fa,
+                                       float2 &fb) {
+     float s0, c0, s1, c1;
+     __sincosf(ph0, &s0, &c0);
+     __sincosf(ph1, &s1, &c1);
+     fa.x = fmaf(x0.x, c0, fmaf(x0.y, s0, fmaf(x1.x, c1, x1.y * s1)));
+     fa.y = fmaf(x0.y, c0, fmaf(-x0.x, s0, fmaf(x1.y, c1, -x1.x * s1)));
+     fb.x = fmaf(x0.z, c0, fmaf(x0.w, s0, fmaf(x1.z, c1, x1.w * s1)));
+     fb.y = fmaf(x0.w, c0, fmaf(-x0.z, s0, fmaf(x1.w, c1, -x1.z * s1)));
+}
+
 // DemodSplit over operands interleaved by detector, xab[(slot*Nal + i)*nifo
 // + d] and s2 likewise (the engine's layout): with two detectors a sample's
 // operands are two adjacent 16-byte words and one 8-byte word, each read
@@ -512,14 +526,7 @@ struct DemodSplitILT {
                          // both detectors' rotated operands summed in one
                          // chain of fused multiply-adds per component
                          const float2 ss = __ldg(reinterpret_cast<const float2 *>(s));
-                         const float4 x0 = __ldg(x), x1 = __ldg(x + 1);
-                         float s0, c0, s1, c1;
-                         __sincosf(fmaf(spf, ss.x, pr), &s0, &c0);
-                         __sincosf(fmaf(spf, ss.y, pr), &s1, &c1);
-                         fa.x = fmaf(x0.x, c0, fmaf(x0.y, s0, fmaf(x1.x, c1, x1.y * s1)));
-                         fa.y = fmaf(x0.y, c0, fmaf(-x0.x, s0, fmaf(x1.y, c1, -x1.x * s1)));
-                         fb.x = fmaf(x0.z, c0, fmaf(x0.w, s0, fmaf(x1.z, c1, x1.w * s1)));
-                         fb.y = fmaf(x0.w, c0, fmaf(-x0.z, s0, fmaf(x1.w, c1, -x1.z * s1)));
+                         demod2(__ldg(x), __ldg(x + 1), fmaf(spf, ss.x, pr), fmaf(spf, ss.y, pr), fa, fb);
                     } else if (nf == 1) {
                          DemodSplit::rot(__ldg(x), fmaf(spf, __ldg(s), pr), fa, fb);
                     } else {
@@ -611,15 +618,10 @@ struct DemodSplitStaged {
                          const double kk = rint(ph * INV_TWO_PI);
                          const float pr = (float)fma(-kk, TWO_PI, ph);
                          const int e0 = (t * LINES + c) * nifo;
-                         if (nifo <= 2) {
+                         if (nifo == 2) {
+                              demod2(X[e0], X[e0 + 1], fmaf(spf, S2[e0], pr), fmaf(spf, S2[e0 + 1], pr), fa, fb);
+                         } else if (nifo == 1) {
                               DemodSplit::rot(X[e0], fmaf(spf, S2[e0], pr), fa, fb);
-                              if (nifo == 2) {
-                                   const int e1 = e0 + 1;
-                                   float2 pa, pb;
-                                   DemodSplit::rot(X[e1], fmaf(spf, S2[e1], pr), pa, pb);
-                                   fa = cadd(fa, pa);
-                                   fb = cadd(fb, pb);
-                              }
                          } else {
                               CompSum ar, ai, br, bi;
                               for (int d = 0; d < nifo; d++) {

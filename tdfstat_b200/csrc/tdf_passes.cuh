@@ -21,15 +21,9 @@ namespace tdf {
 template <int L>
 constexpr int pass_threads() { return L / 8 * LINES; }
 
-// two FP32 arrays use the interleaved line buffer (LineGeom2)
-template <typename T, int NA>
-__host__ __device__ constexpr bool interleaved2() { return NA == 2 && sizeof(T) == 4; }
-
 template <typename T, int L, int NA>
 constexpr size_t pass_smem_bytes() {
-     const size_t planar = sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
-     const size_t il = sizeof(cx<T>) * L + 16 * (size_t)LINES * LineGeom2<L>::STRIDE;
-     return interleaved2<T, NA>() && il > planar ? il : planar;
+     return sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
 }
 
 // resident CTAs per SM the FP32 passes are compiled for (register cap):
@@ -88,15 +82,11 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
                                       reinterpret_cast<uint64_t *>(smem_raw + pro.bar_off));
      else
           pro.template load<L>(v, b, n2, t);
-     __syncthreads();
-     if constexpr (interleaved2<T, NA>()) {
-          line_fft2<L, SIGN>(v, reinterpret_cast<float4 *>(lines) + c * LineGeom2<L>::STRIDE, tw, t);
-     } else {
-          cx<T> *s[NA];
+     cx<T> *s[NA];
 #pragma unroll
-          for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
-          line_fft<T, L, SIGN, NA>(v, s, tw, t);
-     }
+     for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
+     __syncthreads();
+     line_fft<T, L, SIGN, NA>(v, s, tw, t);
      if constexpr (has_tables<Epi>::value)
           epi.template store<L>(v, b, n2, t, smem_raw);
      else
@@ -124,14 +114,10 @@ __global__ void __launch_bounds__(pass_threads<L>(), (row_min_blocks<T, L>())) k
           src.template load<L>(v, b, k1b + c, t);
           load_table<T>(tw, twline, L);
      }
-     __syncthreads();
-     if constexpr (interleaved2<T, NA>()) {
-          line_fft2<L, SIGN>(v, reinterpret_cast<float4 *>(lines) + c * LineGeom2<L>::STRIDE, tw, t);
-     } else {
 #pragma unroll
-          for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
-          line_fft<T, L, SIGN, NA>(v, s, tw, t);
-     }
+     for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
+     __syncthreads();
+     line_fft<T, L, SIGN, NA>(v, s, tw, t);
      epi.template store<L>(v, b, k1b + c, t);
 }
 

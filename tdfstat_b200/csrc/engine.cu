@@ -119,9 +119,9 @@ static bool is_sky_kernel(const void *k) {
      return std::find(g_sky_kernels.begin(), g_sky_kernels.end(), k) != g_sky_kernels.end();
 }
 
-template <typename T, int L, int SIGN, int NA, class Pro, class Epi, int LN = LINES>
+template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
 static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T> *tw, cudaStream_t st) {
-     size_t smem = pass_smem_bytes<T, L, NA, LN>();
+     size_t smem = pass_smem_bytes<T, L, NA>();
      if constexpr (is_staged<Pro>::value) smem = pro.smem;
      Epi epi = epi_in;
      if constexpr (has_tables<Epi>::value) {
@@ -130,10 +130,10 @@ static int launch_col_L(dim3 grid, const Pro &pro, const Epi &epi_in, const cx<T
           epi.tab_off = (unsigned)smem;
           smem += Epi::template table_bytes<L>(epi.N2);
      }
-     auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi, LN>;
+     auto kern = k_colpass<T, L, SIGN, NA, Pro, Epi>;
      if constexpr (NA == 1) register_sky_kernel((const void *)kern);
      TRY(set_smem(kern, smem));
-     kern<<<grid, pass_threads<L, LN>(), smem, st>>>(pro, epi, tw);
+     kern<<<grid, pass_threads<L>(), smem, st>>>(pro, epi, tw);
      CUCHK(cudaGetLastError());
      return TDF_OK;
 }
@@ -417,7 +417,6 @@ struct tdf_engine {
      uint64_t graph_tick = 0;
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
      bool graph_prio = true;   // TDF_GRAPH_PRIORITY=0 leaves captured kernel nodes at their default priority
-     int col_lines = 8;        // columns per CTA of the split form's 512-point column pass (TDF_COL_LINES=4|8)
      bool row_bulk = true;     // row passes fetch their rows by bulk copies (TDF_ROW_BULK=0: per thread)
      // split form: the row pass keeps F on the chip and hands over only the
      // candidates and the edge bins of its runs (TDF_FULL_F=1: full F ring);
@@ -937,24 +936,17 @@ static int group_templates(const tdf_engine *e) { return std::max(1, e->Gt / e->
 // time for the transform lengths of the benchmark sizes (nfftf 2^15 .. 2^18,
 // two detectors); every other case takes the same policies with the
 // geometry read at run time.
-template <int L, int N2C, int LN = LINES>
+template <int L, int N2C>
 static int launch_split_col_c(dim3 grid, const DemodSplitIL &p, const StoreFourstepG<0> &g, const float2 *tw,
                               cudaStream_t st) {
      DemodSplitILT<N2C, 2> pro{p.xab, p.s2, p.tp, p.N, p.N2, p.Nal, p.nifo};
      StoreFourstepG<N2C> epi{g.y, g.w0, g.ws, g.N2, g.N};
-     return launch_col_L<float, L, -1, 2, DemodSplitILT<N2C, 2>, StoreFourstepG<N2C>, LN>(grid, pro, epi, tw, st);
+     return launch_col_L<float, L, -1, 2>(grid, pro, epi, tw, st);
 }
 
-// col_lines: columns per CTA of the 512-point column passes (8: 512
-// threads, 2 CTAs per SM; 4: 256 threads, 4 CTAs per SM)
-static int launch_split_col(int nifo, int N1, int N2, int col_lines, dim3 grid, const DemodSplitIL &pro,
-                            const StoreFourstepG<0> &epi, const float2 *tw, cudaStream_t st) {
+static int launch_split_col(int nifo, int N1, int N2, dim3 grid, const DemodSplitIL &pro, const StoreFourstepG<0> &epi,
+                            const float2 *tw, cudaStream_t st) {
      if (nifo == 2) {
-          if (N1 == 512 && col_lines == 4) {
-               const dim3 g4(N2 / 4, grid.y);
-               if (N2 == 512) return launch_split_col_c<512, 512, 4>(g4, pro, epi, tw, st);
-               if (N2 == 256) return launch_split_col_c<512, 256, 4>(g4, pro, epi, tw, st);
-          }
           if (N1 == 512 && N2 == 512) return launch_split_col_c<512, 512>(grid, pro, epi, tw, st);
           if (N1 == 512 && N2 == 256) return launch_split_col_c<512, 256>(grid, pro, epi, tw, st);
           if (N1 == 256 && N2 == 256) return launch_split_col_c<256, 256>(grid, pro, epi, tw, st);
@@ -1023,7 +1015,7 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
           } else {
                DemodSplitIL pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal,
                                 e->nifo};
-               TRY(launch_split_col(e->nifo, t.N1, t.N2, e->col_lines, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st));
+               TRY(launch_split_col(e->nifo, t.N1, t.N2, dim3(t.N2 / LINES, nt), pro, epi, t.l1(), st));
           }
      } else {
           StoreFourstep<T, -1, 2> epi{Ln.Ybuf.as<cx<T>>(), t.h(), t.o(), t.N2, e->nfftf};
@@ -1759,8 +1751,6 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
      const char *gr = getenv("TDF_GRAPHS");
      if (gr && gr[0] == '0') e->use_graphs = false;
-     const char *cl = getenv("TDF_COL_LINES");
-     if (cl && atoi(cl) == 4) e->col_lines = 4;
      const char *gp = getenv("TDF_GRAPH_PRIORITY");
      if (gp && gp[0] == '0') e->graph_prio = false;
      const char *ff = getenv("TDF_FULL_F");

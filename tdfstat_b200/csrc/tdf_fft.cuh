@@ -106,25 +106,16 @@ __host__ __device__ constexpr int ilog8(int L) { return L >= 512 ? 3 : (L >= 64 
 __host__ __device__ constexpr int ipow8(int p) { return p == 0 ? 1 : 8 * ipow8(p - 1); }
 __device__ __forceinline__ int pad8(int p) { return p + (p >> 3); }
 
-constexpr int LINES = 8;   // lines (columns or rows) per CTA
-
-// LN lines per CTA (8, or 4 for the 256-thread column pass of 512-point
-// lines); lane l works on line l % LN at position t = l / LN.
-template <typename T, int L, int LN = LINES> struct LineGeom {
+template <typename T, int L> struct LineGeom {
      static constexpr int LP = L + L / 8;   // padded line length
-     // bank-spreading line stride.  8-byte elements, 8 lines: a half-warp
-     // is 8 lines x 2 consecutive t, STRIDE == 2 (mod 16); 4 lines: 4 lines
-     // x 4 consecutive t (positions 9t + r, or consecutive), STRIDE == 4
-     // (mod 16).  16-byte elements (8 lines only): a quarter-warp is 8 lines
-     // at one t, STRIDE odd.
-     static_assert(sizeof(cx<T>) == 8 || LN == 8, "16-byte elements use 8 lines per CTA");
-     static constexpr int STRIDE = sizeof(cx<T>) == 8
-                                       ? LP + (((LN == 8 ? 2 : 4) - LP % 16) + 16) % 16
-                                       : LP + (LP % 2 == 0 ? 1 : 0);
+     // bank-spreading line stride: == 2 (mod 16) for 8-byte, odd for 16-byte elements
+     static constexpr int STRIDE = sizeof(cx<T>) == 8 ? LP + ((2 - LP % 16) + 16) % 16 : LP + (LP % 2 == 0 ? 1 : 0);
      static constexpr int NT = L / 8;       // threads per line
      static constexpr int P8 = ilog8(L);    // radix-8 passes
      static constexpr int RL = L / ipow8(ilog8(L));   // last radix (1 = none)
 };
+
+constexpr int LINES = 8;   // lines (columns or rows) per CTA
 
 // Apply the Stockham twiddles of a pass (radix R, span NS) to the butterflies
 // a thread owns, for all NA lines it holds (the twiddles depend only on the

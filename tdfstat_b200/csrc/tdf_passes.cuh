@@ -17,21 +17,21 @@
 
 namespace tdf {
 
-// threads of a pass CTA: L/8 per line, LN lines
-template <int L, int LN = LINES>
-constexpr int pass_threads() { return L / 8 * LN; }
+// threads of a pass CTA: L/8 per line, LINES lines
+template <int L>
+constexpr int pass_threads() { return L / 8 * LINES; }
 
-template <typename T, int L, int NA, int LN = LINES>
+template <typename T, int L, int NA>
 constexpr size_t pass_smem_bytes() {
-     return sizeof(cx<T>) * (L + (size_t)NA * LN * LineGeom<T, L, LN>::STRIDE);
+     return sizeof(cx<T>) * (L + (size_t)NA * LINES * LineGeom<T, L>::STRIDE);
 }
 
 // resident CTAs per SM the FP32 passes are compiled for (register cap):
 // column passes, and row passes (which hold no demodulation operands and fit
 // 64 registers at L <= 256 without spilling)
-template <typename T, int L, int LN = LINES>
+template <typename T, int L>
 constexpr int pass_min_blocks() {
-     return sizeof(T) == 4 ? (LN == 4 && L == 512 ? 4 : (L <= 256 ? 3 : (L == 512 ? 2 : 1))) : 1;
+     return sizeof(T) == 4 ? (L <= 256 ? 3 : (L == 512 ? 2 : 1)) : 1;
 }
 template <typename T, int L>
 constexpr int row_min_blocks() {
@@ -63,18 +63,18 @@ struct has_tables : std::false_type {};
 template <class P>
 struct has_tables<P, std::void_t<decltype(P::kTables)>> : std::integral_constant<bool, P::kTables> {};
 
-template <typename T, int L, int SIGN, int NA, class Pro, class Epi, int LN = LINES>
-__global__ void __launch_bounds__(pass_threads<L, LN>(), (pass_min_blocks<T, L, LN>()))
+template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
+__global__ void __launch_bounds__(pass_threads<L>(), (pass_min_blocks<T, L>()))
 k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
-     using G = LineGeom<T, L, LN>;
+     using G = LineGeom<T, L>;
      extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
      load_table<T>(tw, twline, L);
      if constexpr (has_tables<Epi>::value) epi.template load_tables<L>(smem_raw);
      const int tid = threadIdx.x;
-     const int c = tid % LN, t = tid / LN;
-     const int n2 = blockIdx.x * LN + c;
+     const int c = tid % LINES, t = tid / LINES;
+     const int n2 = blockIdx.x * LINES + c;
      const int b = blockIdx.y;
      cx<T> v[NA][8];
      if constexpr (is_staged<Pro>::value)
@@ -84,7 +84,7 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
           pro.template load<L>(v, b, n2, t);
      cx<T> *s[NA];
 #pragma unroll
-     for (int a = 0; a < NA; a++) s[a] = lines + (a * LN + c) * G::STRIDE;
+     for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
      __syncthreads();
      line_fft<T, L, SIGN, NA>(v, s, tw, t);
      if constexpr (has_tables<Epi>::value)

@@ -162,27 +162,3 @@ def test_sparse_f_store_matches_full_store(golden, monkeypatch, name):
     eng = Engine.from_job(g.job32, form="split")
     _same(_records(eng.search(pm, mm, nn)), ref)
     eng.close()
-
-
-@pytest.mark.parametrize("name", ["cfg2", "cfg3"])
-def test_four_column_ctas_match(monkeypatch, tmp_path, name):
-    """TDF_COL_LINES=4 (the 512-point column pass in CTAs of 4 columns and
-    256 threads) gives the same records, bit for bit, as the default CTAs
-    of 8 columns: one sky point x 21 spindowns at the benchmark sizes
-    (nfftf 2^17 and 2^18, the compile-time geometries)."""
-    from tdfstat_b200.engine import Engine
-    from tdfstat_b200.workloads import Workload
-    wl = Workload(name, str(tmp_path))
-    ip = wl.centre
-    pm, mm, nn = wl.pm[ip:ip + 1], wl.mm[ip:ip + 1], wl.nn[ip:ip + 1]
-    opts = wl.job.search_opts()
-    sst = np.array([opts.spndr[1] - 20], dtype=np.float32)
-    eng = Engine.from_job(wl.job, form="split")
-    ref = _records(eng.search(pm, mm, nn, sst=sst))
-    eng.close()
-    monkeypatch.setenv("TDF_COL_LINES", "4")
-    eng = Engine.from_job(wl.job, form="split")
-    got = _records(eng.search(pm, mm, nn, sst=sst))
-    eng.close()
-    assert len(got[0]) == 21 and sum(len(p) for p in got[1]) > 0
-    _same(got, ref)

@@ -355,7 +355,7 @@ struct tdf_engine {
           DevBuf cand;    // candidate bins of a resolve group (uint2), or the sparse store's records (uint4)
           DevBuf Ebuf;    // sparse F store: edge ring of a resolve group (split form)
      };
-     static constexpr int kMaxLanes = 4;
+     static constexpr int kMaxLanes = 6;
      Lane ln[kMaxLanes];
      int nlanes = 3;                                  // TDF_LANES=n (1..4)
      cudaStream_t lane_own[kMaxLanes] = {};          // streams of lanes 1.. (lane 0 runs on `stream`)
@@ -1744,7 +1744,7 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (max_sky_batch > 0) e->Bs = max_sky_batch;
      const char *tc = getenv("TDF_TEMPLATES_PER_CHUNK");
      if (tc && atoi(tc) > 0) e->Tc = atoi(tc);
-     e->TcMax = std::max(48, e->Tc);
+     e->TcMax = std::max(96, e->Tc);
      const char *ov = getenv("TDF_SKY_OVERLAP");
      if (ov && ov[0] == '0') e->overlap = false;
      const char *nl = getenv("TDF_LANES");
@@ -2286,15 +2286,15 @@ static int autotune_time(tdf_engine *e, int npts, const int32_t *pm, const float
      return TDF_OK;
 }
 
-// Coordinate search: the templates per chunk (6..48) at the current lanes and
-// group size, then the lanes (2..4) at the best chunk size, then the
+// Coordinate search: the templates per chunk (6..96) at the current lanes and
+// group size, then the lanes (2..6) at the best chunk size, then the
 // templates per resolve group (32, 64, 128).
 int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float *mm, const float *nn,
                         int32_t *best) {
      if (!e) return set_error(TDF_ERR_INVALID, "null engine");
      CUCHK(cudaSetDevice(e->dev));
-     static const int tcs[] = {6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 37, 41, 48};
-     static const int lanes[] = {2, 3, 4};
+     static const int tcs[] = {6, 8, 10, 12, 14, 16, 20, 24, 28, 32, 37, 41, 48, 64, 80, 96};
+     static const int lanes[] = {2, 3, 4, 5, 6};
      static const int gts[] = {32, 64, 128};
      cudaEvent_t a, b;
      CUCHK(cudaEventCreate(&a));

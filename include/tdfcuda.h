@@ -332,8 +332,8 @@ int tdf_engine_set_stream(tdf_engine *e, void *stream);
 
 /* Chooses the spindown stage's launch configuration by timing device-only
    passes over these points: the templates per chunk (one column-pass and
-   one row-pass launch each; 6..48), then the lanes (concurrent streams with
-   their own buffers; 2..4), then the templates per resolve group (the
+   one row-pass launch each; 6..96), then the lanes (concurrent streams with
+   their own buffers; 2..6), then the templates per resolve group (the
    trigger-selection launch's share; 32, 64, 128), each at the best of the
    previous choices, and keeps the fastest in the engine; *best (may be
    NULL) receives the templates per chunk, tdf_engine_get_tuning() all
@@ -345,7 +345,7 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
 int tdf_engine_get_tuning(tdf_engine *e, int32_t *templates_per_chunk, int32_t *lanes, int32_t *group_templates);
 
 /* Templates per chunk of the spindown stage (one column-pass and one
-   row-pass launch each): get, and set to 1..48 (TDF_ERR_INVALID otherwise).
+   row-pass launch each): get, and set to 1..96 (TDF_ERR_INVALID otherwise).
    tdf_engine_autotune() chooses it; a set value holds until the next
    autotune.  Extension of this library: job_core() has no chunking. */
 int tdf_engine_get_templates_per_chunk(tdf_engine *e, int32_t *tc);

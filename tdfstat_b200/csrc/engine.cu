@@ -357,6 +357,7 @@ struct tdf_engine {
      };
      static constexpr int kMaxLanes = 6;
      Lane ln[kMaxLanes];
+     int lanes_alloc = kMaxLanes;   // lanes with buffers and streams (TDF_LANES fixes it to that count)
      int nlanes = 3;                                  // TDF_LANES=n (1..4)
      cudaStream_t lane_own[kMaxLanes] = {};          // streams of lanes 1.. (lane 0 runs on `stream`)
      cudaEvent_t fork_ev = nullptr, join_ev[kMaxLanes] = {};
@@ -671,7 +672,7 @@ static int engine_alloc(tdf_engine *e) {
      const size_t rsz = e->form == TDF_FORM_SPLIT ? sizeof(float) : sizeof(double);
      const size_t G = (size_t)std::max(tdf_engine::kGtMax, Tc);   // templates per resolve group at most
      e->cand_cap = (unsigned)G * 4096u;
-     for (int l = 0; l < tdf_engine::kMaxLanes; l++) {   // every lane: the autotuner may use them all
+     for (int l = 0; l < e->lanes_alloc; l++) {   // every lane the autotuner may use
           tdf_engine::Lane &L = e->ln[l];
           TRY(L.Ybuf.alloc((size_t)Tc * 2 * e->nfftf * csz));
           TRY(L.Fbuf.alloc(G * e->nF * rsz));
@@ -1324,7 +1325,7 @@ static int search_core(tdf_engine *e, int npts, const int32_t *pm, const float *
           CUCHK(cudaStreamSynchronize(e->sky_stream));
           CUCHK(cudaStreamSynchronize(e->stream));
           for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
-          for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+          for (int l = 0; l < e->lanes_alloc; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
           int pending[2] = {0, 0};
           bool over = false, need_full = false;
           size_t b = 0;
@@ -1441,7 +1442,7 @@ static void autotune_cache_lookup(tdf_engine *e) {
           if (strncmp(line, key.c_str(), key.size()) == 0 && line[key.size()] == ' ') {
                int tc = 0, lanes = 0, gt = 0;
                if (sscanf(line + key.size() + 1, "%d %d %d", &tc, &lanes, &gt) == 3 && tc > 0 && tc <= e->TcMax &&
-                   lanes >= 1 && lanes <= tdf_engine::kMaxLanes && gt >= 1 && gt <= tdf_engine::kGtMax) {
+                   lanes >= 1 && lanes <= e->lanes_alloc && gt >= 1 && gt <= tdf_engine::kGtMax) {
                     e->Tc = tc;
                     e->nlanes = lanes;
                     e->Gt = gt;
@@ -1544,7 +1545,7 @@ static int enqueue_plan(tdf_engine *e, const std::vector<PlanBatch> &pb) {
      CUCHK(cudaGetLastError());
      e->launches++;
      for (int s = 0; s < 2; s++) CUCHK(cudaMemsetAsync(e->counters[s].p, 0, 2 * sizeof(unsigned long long), e->stream));
-     for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+     for (int l = 0; l < e->lanes_alloc; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
      // the sky stream's first work of the plan follows this point of the engine stream
      CUCHK(cudaEventRecord(e->plan_ev, e->stream));
      for (size_t i = 0; i < pb.size(); i++) {
@@ -1744,11 +1745,17 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (max_sky_batch > 0) e->Bs = max_sky_batch;
      const char *tc = getenv("TDF_TEMPLATES_PER_CHUNK");
      if (tc && atoi(tc) > 0) e->Tc = atoi(tc);
-     e->TcMax = std::max(96, e->Tc);
+     // buffers for chunks up to 96 templates (the autotuner's range), or for
+     // exactly the fixed chunk size TDF_TEMPLATES_PER_CHUNK asks for
+     e->TcMax = (tc && atoi(tc) > 0) ? e->Tc : std::max(96, e->Tc);
      const char *ov = getenv("TDF_SKY_OVERLAP");
      if (ov && ov[0] == '0') e->overlap = false;
      const char *nl = getenv("TDF_LANES");
-     if (nl && atoi(nl) > 0) e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
+     if (nl && atoi(nl) > 0) {
+          // a fixed lane count: buffers and streams for that many only
+          e->nlanes = std::min(atoi(nl), (int)tdf_engine::kMaxLanes);
+          e->lanes_alloc = e->nlanes;
+     }
      const char *gr = getenv("TDF_GRAPHS");
      if (gr && gr[0] == '0') e->use_graphs = false;
      const char *gp = getenv("TDF_GRAPH_PRIORITY");
@@ -1771,7 +1778,7 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (ce == cudaSuccess) ce = cudaStreamCreateWithPriority(&e->sky_stream, cudaStreamNonBlocking, prio_low);
      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
      if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->plan_ev, cudaEventDisableTiming);
-     for (int l = 1; l < tdf_engine::kMaxLanes && ce == cudaSuccess; l++) {
+     for (int l = 1; l < e->lanes_alloc && ce == cudaSuccess; l++) {
           ce = cudaStreamCreateWithPriority(&e->lane_own[l], cudaStreamNonBlocking, prio_high);
           if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join_ev[l], cudaEventDisableTiming);
      }
@@ -2221,7 +2228,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      CUCHK(cudaStreamWaitEvent(e->stream, e->sky_done[0], 0));
      CUCHK(cudaMemcpyAsync(e->tparam.p, e->h_tp[0], sizeof(TmplParam), cudaMemcpyHostToDevice, e->stream));
      CUCHK(cudaMemsetAsync(e->counters[0].p, 0, 2 * sizeof(unsigned long long), e->stream));
-     for (int l = 0; l < tdf_engine::kMaxLanes; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
+     for (int l = 0; l < e->lanes_alloc; l++) CUCHK(cudaMemsetAsync(e->ln[l].tcnt.p, 0, e->ln[l].tcnt.bytes, e->stream));
      e->sparse_now = false;   // the spectrum itself is the output: the full F store
      TRY(run_templates(e, e->tparam.as<TmplParam>(), 1));
      CUCHK(cudaMemcpyAsync(e->h_cnt, e->counters[0].p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
@@ -2314,7 +2321,7 @@ int tdf_engine_autotune(tdf_engine *e, int npts, const int32_t *pm, const float 
      }
      e->Tc = btc;
      for (int l : lanes) {
-          if (st != TDF_OK || l == bl) continue;
+          if (st != TDF_OK || l == bl || l > e->lanes_alloc) continue;
           e->nlanes = l;
           st = autotune_time(e, npts, pm, mm, nn, a, b, &ms);
           if (st == TDF_OK && ms < best_ms) {

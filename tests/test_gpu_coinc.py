@@ -6,8 +6,8 @@ FP64 form: the records equal the reference's, so every coincidence and its
 members must match (values to float rounding).  Split form: F differs from
 the reference by ~1e-6, which can swap which of two nearly equal triggers is
 the loudest of a cell; at least 99% of the coincidences must have the
-reference's members, the leading three of every shift the reference's
-values (1e-4) in order, and the counts stay within 1%."""
+reference's members, 98% also its values (1e-4), the leading three of every
+shift in order, and the counts stay within 1%."""
 import numpy as np
 import pytest
 
@@ -47,10 +47,8 @@ def test_fp64_gpu_coincidences_match_reference(c1, key):
 def test_split_gpu_coincidences_close_to_reference(c1):
     """Every shift: the count within 1%, at least 99% of the reference's
     coincidences found with the same members (segments and template
-    numbers), and the leading three in the same order with their average
-    SNR and frequency within 1e-4.  (A member's loudest trigger in a cell
-    can differ where the split form's F moves a trigger across a threshold
-    or neighbour tie, which changes that coincidence's averages.)"""
+    numbers), at least 98% also with the reference's average SNR and
+    frequency (1e-4), and the leading three in the same order."""
     segs = _gpu_segments(c1, "split")
     got, seginfo = coincidences(CoincOptions(**c1.cc["opts"]["a"]), segs)
     total = same = same_v = 0
@@ -58,18 +56,25 @@ def test_split_gpu_coincidences_close_to_reference(c1):
         si, w, vals, cseg, trig, ntrig = c1.expected("a", ish)
         mine = [c for c in got if c.shift == ish]
         assert abs(len(mine) - len(w)) <= max(2, 0.01 * len(w))
+        # the same members (segment, template) can form several
+        # coincidences (other frequency cells): the reference's values per
+        # member set, each used once
         ref = {}
         m = 0
         for k in range(len(w)):
             key = tuple(zip(cseg[m:m + w[k]].tolist(), trig[m:m + w[k]].tolist()))
-            ref[key] = vals[k]
+            ref.setdefault(key, []).append(np.asarray(vals[k][:2], dtype=np.float64))
             m += int(w[k])
         for c in mine:
             key = tuple(zip(np.asarray(c.cseg).tolist(), np.asarray(c.trig).tolist()))
-            if key in ref:
+            if key in ref and ref[key]:
                 same += 1
-                if np.allclose([c.avg_snr, c.avg_f], ref[key][:2], rtol=1e-4, atol=0):
-                    same_v += 1
+                got_v = np.array([c.avg_snr, c.avg_f], dtype=np.float64)
+                for i, rv in enumerate(ref[key]):
+                    if np.allclose(got_v, rv, rtol=1e-4, atol=0):
+                        same_v += 1
+                        del ref[key][i]
+                        break
         total += len(w)
         for k in range(min(3, len(w))):     # the leading coincidences, in order
             c = mine[k]
@@ -80,3 +85,4 @@ def test_split_gpu_coincidences_close_to_reference(c1):
     print("split-form coincidences with the reference's members: %d of %d, of them %d with its average SNR and "
           "frequency (1e-4)" % (same, total, same_v))
     assert same >= 0.99 * total
+    assert same_v >= 0.98 * total

@@ -906,12 +906,10 @@ static int run_sky_stage(tdf_engine *e, int npts, const SkyParam *dsky = nullptr
      e->launches += 4;
      // spline: B0 (samples) -> B1 (u) -> B2 (second derivatives)
      {
-          const int K = 64, Wu = 48;   // chunk per thread, warm-up steps
-          const int nch = (e->n2N + K - 1) / K;
-          dim3 g((nch + 127) / 128, 2 * Q);
-          k_spline_fwd<<<g, 128, 0, st>>>(e->B0.as<double2>(), e->B1.as<double2>(), ws, e->pco.as<double>(), e->n2N, K, Wu);
+          dim3 g((e->n2N + SPL_TILE - 1) / SPL_TILE, 2 * Q);
+          k_spline_fwd<<<g, SPL_T, 0, st>>>(e->B0.as<double2>(), e->B1.as<double2>(), ws, e->pco.as<double>(), e->n2N);
           CUCHK(cudaGetLastError());
-          k_spline_bwd<<<g, 128, 0, st>>>(e->B1.as<double2>(), e->B2.as<double2>(), ws, e->gco.as<double>(), e->n2N, K, Wu);
+          k_spline_bwd<<<g, SPL_T, 0, st>>>(e->B1.as<double2>(), e->B2.as<double2>(), ws, e->gco.as<double>(), e->n2N);
           CUCHK(cudaGetLastError());
      }
      k_splint<<<dim3((e->N + 255) / 256, Q), 256, 0, st>>>(

@@ -256,28 +256,53 @@ __global__ void __launch_bounds__(256) k_sky_sums(const double *__restrict__ par
      }
 }
 
-// Forward sweep of the natural spline (auxi.c:102-111), u[i] for i in [1, n-2]
-// (u[0] = 0).  Thread = chunk of K indices, started W indices early from
-// u = 0: the recurrence contracts by |0.5*invp| ~ 0.27 per step, so the
-// start-up error is below 1e-27 of |u| after W = 48 steps.
-// grid (ceil(nchunk/128), 2*Q), 128 threads
-__global__ void k_spline_fwd(const double2 *__restrict__ Z, double2 *__restrict__ U, size_t stride,
-                             const double *__restrict__ pco, int n, int K, int Wu)
+// The natural-spline sweeps (auxi.c:102-115) as blocked recurrences: a
+// thread computes a chunk of SPL_K consecutive indices, started SPL_W indices
+// early from zero -- both recurrences contract by |0.5*invp| ~ 0.27 per step,
+// so the start-up error is below 1e-27 of the values after 48 steps and the
+// results are those of one sequential sweep.  A CTA of SPL_T threads stages
+// its tile of the inputs (and the warm-up margin) in shared memory with
+// coalesced loads; lane j then reads index j*SPL_K + r, and one pad word per
+// 16 elements puts the lanes of a wavefront on distinct banks.
+constexpr int SPL_T = 64;                  // threads per CTA
+constexpr int SPL_K = 16;                  // indices per thread
+constexpr int SPL_W = 48;                  // warm-up steps
+constexpr int SPL_TILE = SPL_T * SPL_K;    // indices per CTA
+__device__ __forceinline__ int spl_pad(int s) { return s + (s >> 4); }
+
+// Forward sweep (auxi.c:102-111), u[i] for i in [1, n-2] (u[0] = 0).
+// grid (ceil(n/SPL_TILE), 2*Q), SPL_T threads
+__global__ void __launch_bounds__(SPL_T) k_spline_fwd(const double2 *__restrict__ Z, double2 *__restrict__ U,
+                                                      size_t stride, const double *__restrict__ pco, int n)
 {
+     constexpr int S = SPL_TILE + SPL_W + 2;   // staged samples: [tile0 - W - 1, tile0 + TILE + 1)
+     constexpr int P = SPL_TILE + SPL_W;       // staged factors:  [tile0 - W, tile0 + TILE)
+     __shared__ double2 ys[S + S / 16 + 1];
+     __shared__ double ps[P + P / 16 + 1];
      const int arr = blockIdx.y;
-     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-     const int lo = c * K;
-     if (lo >= n) return;
      const double2 *y = Z + (size_t)arr * stride;
      double2 *u = U + (size_t)arr * stride;
-     const int hi = min(n - 1, lo + K);
+     const int tile0 = blockIdx.x * SPL_TILE;
+     const int yb = tile0 - SPL_W - 1, pb = tile0 - SPL_W;
+     for (int k = threadIdx.x; k < S; k += SPL_T) {
+          const int i = yb + k;
+          if (i >= 0 && i < n) ys[spl_pad(k)] = y[i];
+     }
+     for (int k = threadIdx.x; k < P; k += SPL_T) {
+          const int i = pb + k;
+          if (i >= 0 && i < n) ps[spl_pad(k)] = pco[i];
+     }
+     __syncthreads();
+     const int lo = tile0 + threadIdx.x * SPL_K;
+     if (lo >= n) return;
+     const int hi = min(n - 1, lo + SPL_K);
      if (lo == 0) u[0] = make_double2(0., 0.);
-     int i0 = max(1, lo - Wu);
+     const int i0 = max(1, lo - SPL_W);
      double ur = 0., ui = 0.;
-     double2 ym = y[i0 - 1], y0 = y[i0];
+     double2 ym = ys[spl_pad(i0 - 1 - yb)], y0 = ys[spl_pad(i0 - yb)];
      for (int i = i0; i < hi; i++) {
-          const double2 yp = y[i + 1];
-          const double p = pco[i];
+          const double2 yp = ys[spl_pad(i + 1 - yb)];
+          const double p = ps[spl_pad(i - pb)];
           const double dr = ym.x - 2. * y0.x + yp.x;
           const double dI = ym.y - 2. * y0.y + yp.y;
           ur = (-.5 * ur + 3. * dr) * p;
@@ -288,24 +313,36 @@ __global__ void k_spline_fwd(const double2 *__restrict__ Z, double2 *__restrict_
      }
 }
 
-// Back substitution (auxi.c:112-115): y2[n-1] = 0, y2[k] = g[k]*y2[k+1] + u[k].
-// Thread = chunk of K indices, started W indices late from y2 = 0.
-__global__ void k_spline_bwd(const double2 *__restrict__ U, double2 *__restrict__ Y2, size_t stride,
-                             const double *__restrict__ gco, int n, int K, int Wu)
+// Back substitution (auxi.c:112-115): y2[n-1] = 0, y2[k] = g[k]*y2[k+1] + u[k];
+// a thread's chunk is started SPL_W indices late from y2 = 0.
+// grid (ceil(n/SPL_TILE), 2*Q), SPL_T threads
+__global__ void __launch_bounds__(SPL_T) k_spline_bwd(const double2 *__restrict__ U, double2 *__restrict__ Y2,
+                                                      size_t stride, const double *__restrict__ gco, int n)
 {
+     constexpr int S = SPL_TILE + SPL_W;       // staged: [tile0, tile0 + TILE + W)
+     __shared__ double2 us[S + S / 16 + 1];
+     __shared__ double gs[S + S / 16 + 1];
      const int arr = blockIdx.y;
-     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-     const int lo = c * K;
-     if (lo >= n) return;
      const double2 *u = U + (size_t)arr * stride;
      double2 *y2 = Y2 + (size_t)arr * stride;
-     const int hi = min(n, lo + K);
-     const int ks = min(n - 1, hi + Wu);
+     const int tile0 = blockIdx.x * SPL_TILE;
+     for (int k = threadIdx.x; k < S; k += SPL_T) {
+          const int i = tile0 + k;
+          if (i < n) {
+               us[spl_pad(k)] = u[i];
+               gs[spl_pad(k)] = gco[i];
+          }
+     }
+     __syncthreads();
+     const int lo = tile0 + threadIdx.x * SPL_K;
+     if (lo >= n) return;
+     const int hi = min(n, lo + SPL_K);
+     const int ks = min(n - 1, hi + SPL_W);
      if (ks == n - 1 && ks < hi) y2[n - 1] = make_double2(0., 0.);
      double yr = 0., yi = 0.;
      for (int k = ks - 1; k >= lo; k--) {
-          const double g = gco[k];
-          const double2 uk = u[k];
+          const double g = gs[spl_pad(k - tile0)];
+          const double2 uk = us[spl_pad(k - tile0)];
           yr = g * yr + uk.x;
           yi = g * yi + uk.y;
           if (k < hi) y2[k] = make_double2(yr, yi);

@@ -108,6 +108,15 @@ def test_invalid_arguments(lib):
     assert lib.tdf_check_bounded_wait(0, 0, C.byref(st)) == _abi.TDF_ERR_INVALID
     assert lib.tdf_check_bounded_wait(0, 1000, None) == _abi.TDF_ERR_INVALID
     assert lib.tdf_check_bounded_wait(0, 1000, C.byref(st)) == _abi.TDF_ERR_NO_DEVICE
+    # the segment-slot and tuning entries check their arguments before any device work
+    slot = C.c_int32(0)
+    assert lib.tdf_engine_add_segment(None, C.byref(seg), C.byref(slot)) == _abi.TDF_ERR_INVALID
+    assert lib.tdf_engine_upload_segment(None, 0, C.byref(seg)) == _abi.TDF_ERR_INVALID
+    n = C.c_int64(0)
+    assert lib.tdf_search_segments_device(None, 0, None, None, None, None, None, C.byref(n),
+                                          C.byref(n)) == _abi.TDF_ERR_INVALID
+    assert lib.tdf_engine_get_tuning(None, None, None, None) == _abi.TDF_ERR_INVALID
+    assert lib.tdf_engine_segment_count(None, None) == _abi.TDF_ERR_INVALID
 
 
 def test_frequency_range_below_bin_zero_is_refused(lib, tmp_path):

@@ -83,11 +83,11 @@ def test_records_do_not_depend_on_chunk_size(golden):
     pm, mm, nn = g.job32.sky_points()
     eng = Engine.from_job(g.job32, form="split")
     ref = _records(eng.search(pm, mm, nn))
-    for tc in (1, 3, 17, 48):
+    for tc in (1, 3, 17, 48, 96):
         eng.templates_per_chunk = tc
         assert eng.templates_per_chunk == tc
         _same(_records(eng.search(pm, mm, nn)), ref)
-    for bad in (0, 49):
+    for bad in (0, 97):
         with pytest.raises(TdfError):
             eng.templates_per_chunk = bad
     eng.close()

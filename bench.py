@@ -351,7 +351,9 @@ def run_tdf(args, rank, world, local_rank):
                 achieved = per_launch_bytes / avg_s / 1e9
                 roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                         "frac": round(achieved / peak, 4), "traffic": None,
-                        "kernel": "k_colpass (demodulation + first FFT pass)",
+                        "kernel": ("k_spinpass (demodulation + both FFT passes + F, one ordered launch)"
+                                   if col_n and not ktimes.get("rowpass_launches")
+                                   else "k_colpass (demodulation + first FFT pass)"),
                         "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                         "algorithmic_bytes_per_template": bt,
                         "kernel_ms": {k: round(v, 3) for k, v in ktimes.items() if k.endswith("_ms")},

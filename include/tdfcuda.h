@@ -107,14 +107,17 @@ typedef struct tdf_record {
 
 typedef struct tdf_engine tdf_engine;
 
-/* Bit set in a kernel's error word when a bounded wait on an asynchronous
-   copy gave up (the search then returns TDF_ERR_CUDA with a message). */
+/* Bits set in a kernel's error word when a bounded wait gave up (the search
+   then returns TDF_ERR_CUDA with a message): a wait on an asynchronous copy,
+   and a fused pass's row block waiting for its template's column blocks. */
 #define TDF_WAIT_TIMEOUT_BIT 2u
+#define TDF_ORDER_TIMEOUT_BIT 8u
 
 /* Health check of the bounded waits: one warp on `device` waits, `probes`
-   probes at most (1..2^20), on a barrier whose copy never arrives, and
-   returns; *status receives the kernel's error word (TDF_WAIT_TIMEOUT_BIT
-   set when the wait gave up, as it must).  The device stays usable. */
+   probes at most (1..2^20), on a barrier whose copy never arrives, then one
+   thread on a block count that nothing raises, and returns; *status receives
+   the kernel's error word (TDF_WAIT_TIMEOUT_BIT and TDF_ORDER_TIMEOUT_BIT
+   set when the waits gave up, as they must).  The device stays usable. */
 int tdf_check_bounded_wait(int device, int32_t probes, uint32_t *status);
 
 const char *tdf_status_string(int status);
@@ -357,8 +360,9 @@ int tdf_engine_launch_count(tdf_engine *e, int64_t *count);
 /* Per-kernel device time, measured with CUDA events recorded on the
    engine's stream around each launch while timing is on. */
 typedef struct tdf_kernel_times {
-     double colpass_ms;          /* demodulation + first FFT pass */
-     double rowpass_ms;          /* second FFT pass + F-statistic */
+     double colpass_ms;          /* demodulation + first FFT pass (with the fused
+                                    passes: the whole k_spinpass launch) */
+     double rowpass_ms;          /* second FFT pass + F-statistic (0 when fused) */
      double threshold_ms;        /* local maxima, veto, trigger append */
      double sky_ms;              /* whole sky stage */
      int64_t colpass_launches, rowpass_launches, threshold_launches, sky_batches;

@@ -354,6 +354,7 @@ struct tdf_engine {
           DevBuf tcnt;    // per-template trigger counts + candidate count
           DevBuf cand;    // candidate bins of a resolve group (uint2), or the sparse store's records (uint4)
           DevBuf Ebuf;    // sparse F store: edge ring of a resolve group (split form)
+          DevBuf ctl;     // fused pass order: tickets, finished CTAs, column blocks done per template
      };
      static constexpr int kMaxLanes = 6;
      Lane ln[kMaxLanes];
@@ -419,6 +420,14 @@ struct tdf_engine {
      bool use_graphs = true;   // TDF_GRAPHS=0 launches every kernel from the host
      bool graph_prio = true;   // TDF_GRAPH_PRIORITY=0 leaves captured kernel nodes at their default priority
      bool row_bulk = true;     // row passes fetch their rows by bulk copies (TDF_ROW_BULK=0: per thread)
+     // split form, N1 = N2: TDF_FUSED_PASSES=1 runs the column and row
+     // passes of a chunk as one ordered launch of persistent CTAs
+     // (k_spinpass), a template's rows fuse_lag templates behind its
+     // columns (TDF_FUSE_LAG=n).  Off by default: its spectra stay in L2,
+     // but each row block's wait and the publishing fences sit on the CTA's
+     // critical path, and it measured ~10% slower than the two launches.
+     bool fused = false;
+     int fuse_lag = 3;
      // split form: the row pass keeps F on the chip and hands over only the
      // candidates and the edge bins of its runs (TDF_FULL_F=1: full F ring);
      // blocks_avg, and a batch that needs more of the spectrum, use the full
@@ -682,6 +691,8 @@ static int engine_alloc(tdf_engine *e) {
           TRY(L.cand.alloc(e->cand_cap * sizeof(uint4)));
           // edge ring: 2 floats per (template, row CTA, k2) = nfftf bytes per template
           if (e->form == TDF_FORM_SPLIT) TRY(L.Ebuf.alloc(G * (size_t)e->nfftf));
+          TRY(L.ctl.alloc((2 + (size_t)Tc) * sizeof(unsigned)));
+          CUCHK(cudaMemset(L.ctl.p, 0, L.ctl.bytes));
      }
      TRY(e->linesd.alloc(std::max<size_t>(1, e->lines.size()) * sizeof(double)));
      if (!e->lines.empty())
@@ -981,6 +992,55 @@ static int launch_split_row(int N1, int N2, int fr1, dim3 grid, const RowsYBulk<
      return launch_row<float, -1, 2>(N2, grid, src, epi, tw, st);
 }
 
+// The two split-form passes of nt templates as one ordered launch of
+// persistent CTAs (k_spinpass), for N1 = N2 = L (nfftf 2^16, 2^18) and two
+// detectors; ctl (2 + nt words) is zeroed first, on the same stream.
+template <int L, bool HALF>
+static int launch_spin_c(int nt, int lag, const DemodSplitIL &p, const StoreFourstepG<0> &g, const RowsYBulk<float> &s,
+                         const StoreFstatT<0, false> &f, const float2 *tw, unsigned *ctl, unsigned *err,
+                         cudaStream_t st) {
+     DemodSplitILT<L, 2> pro{p.xab, p.s2, p.tp, p.N, p.N2, p.Nal, p.nifo};
+     StoreFourstepG<L> epic{g.y, g.w0, g.ws, g.N2, g.N};
+     StoreFstatT<L, HALF> epir{f.F, f.tp, f.ab, f.nF, f.fr0, f.fr1, f.N1, f.thr, f.cand, f.cand_cnt, f.cand_cap, f.boff,
+                               f.E, f.scand};
+     RowsYBulk<float> src = s;
+     size_t smem = pass_smem_bytes<float, L, 2>();
+     smem = (smem + 15) / 16 * 16;
+     src.bar_off = (unsigned)smem;
+     smem += 16;
+     SpinOrder o{ctl, err, nt, L / LINES, L / LINES, std::max(1, std::min(lag, nt)), 1 << 20};
+     auto kern = k_spinpass<L, DemodSplitILT<L, 2>, StoreFourstepG<L>, RowsYBulk<float>, StoreFstatT<L, HALF>>;
+     TRY(set_smem(kern, smem));
+     // as many CTAs as are resident at once (queried once per device and variant)
+     static std::mutex mu;
+     static int resident[64] = {};
+     int dev = 0;
+     CUCHK(cudaGetDevice(&dev));
+     int nres;
+     {
+          std::lock_guard<std::mutex> lk(mu);
+          if (dev < 64 && resident[dev] > 0) {
+               nres = resident[dev];
+          } else {
+               int per_sm = 0, nsm = 0;
+               CUCHK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pass_threads<L>(), smem));
+               CUCHK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+               nres = std::max(1, per_sm) * std::max(1, nsm);
+               if (dev < 64) resident[dev] = nres;
+          }
+     }
+     const unsigned items = (unsigned)nt * (unsigned)(o.C + o.R);
+     CUCHK(cudaMemsetAsync(ctl, 0, (2 + (size_t)nt) * sizeof(unsigned), st));
+     kern<<<std::min(items, (unsigned)nres), pass_threads<L>(), smem, st>>>(pro, epic, src, epir, tw, o);
+     CUCHK(cudaGetLastError());
+     return TDF_OK;
+}
+
+// whether the chunk passes of this engine run as one ordered launch
+static bool spin_fused(const tdf_engine *e, int N1, int N2) {
+     return e->fused && !e->staged && e->row_bulk && e->nifo == 2 && N1 == N2 && (N1 == 512 || N1 == 256);
+}
+
 template <typename T>
 static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt) {
      cudaStream_t st = lane_stream(e, l);
@@ -995,6 +1055,37 @@ static int run_chunk(tdf_engine *e, int l, const TmplParam *dtp, int ci, int nt)
      unsigned *tcnt = Ln.tcnt.as<unsigned>();
      size_t tev = e->timing ? timing_begin(e, st) : (size_t)-1;
      if constexpr (std::is_same<T, float>::value) {
+          if (spin_fused(e, t.N1, t.N2)) {
+               StoreFourstepG<0> epi{Ln.Ybuf.as<float2>(), t.base.template as<float2>(), t.step.template as<float2>(),
+                                     t.N2, e->nfftf};
+               DemodSplitIL pro{e->xab[e->cur].as<float4>(), e->s2[e->cur].as<float>(), ctp, e->N, t.N2, e->Nal,
+                                e->nifo};
+               unsigned *errw = reinterpret_cast<unsigned *>(e->counters[e->cur].as<unsigned long long>() + 1);
+               const bool blocks = e->opts.blocks_avg && e->nblk_mu > 0;
+               StoreFstatT<0, false> epi2{Ln.Fbuf.as<float>() + (size_t)boff * e->nF, ctp, e->aabb[e->cur].as<AaBb>(),
+                                          e->nF, e->opts.fr[0], e->opts.fr[1], t.N1, e->opts.thr,
+                                          blocks ? nullptr : Ln.cand.as<uint2>(), tcnt + G, e->cand_cap, boff};
+               if (e->sparse_now) {
+                    epi2.cand = nullptr;
+                    epi2.E = Ln.Ebuf.as<float>();
+                    epi2.scand = Ln.cand.as<uint4>();
+               }
+               RowsYBulk<float> src{Ln.Ybuf.as<float2>(), e->nfftf, t.N2, errw};
+               const bool half = (int64_t)e->opts.fr[1] < (int64_t)t.N1 * t.N2 / 2;
+               unsigned *ctl = Ln.ctl.as<unsigned>();
+               const float2 *tw = t.l1();   // N1 = N2: the row pass's line table is the same
+               int rc;
+               if (t.N1 == 512)
+                    rc = half ? launch_spin_c<512, true>(nt, e->fuse_lag, pro, epi, src, epi2, tw, ctl, errw, st)
+                              : launch_spin_c<512, false>(nt, e->fuse_lag, pro, epi, src, epi2, tw, ctl, errw, st);
+               else
+                    rc = half ? launch_spin_c<256, true>(nt, e->fuse_lag, pro, epi, src, epi2, tw, ctl, errw, st)
+                              : launch_spin_c<256, false>(nt, e->fuse_lag, pro, epi, src, epi2, tw, ctl, errw, st);
+               TRY(rc);
+               if (e->timing) timing_end(e, tev, KT_COL, nt, st);
+               e->launches += 1;   // the memset before it is not a kernel
+               return TDF_OK;
+          }
           StoreFourstepG<0> epi{Ln.Ybuf.as<float2>(), t.base.template as<float2>(), t.step.template as<float2>(), t.N2,
                                 e->nfftf};
           if (e->staged) {
@@ -1253,6 +1344,15 @@ static int ensure_tparam(tdf_engine *e, size_t n) {
      return TDF_OK;
 }
 
+// the error of a kernel error word whose bounded waits gave up, else TDF_OK
+static int wait_error(unsigned errf) {
+     if (errf & ERR_STAGE_TIMEOUT)
+          return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
+     if (errf & ERR_ORDER_TIMEOUT)
+          return set_error(TDF_ERR_CUDA, "spindown stage: a row block's wait for its column blocks gave up");
+     return TDF_OK;
+}
+
 // Waits for the batch last run in `slot`, checks its flags and collects its
 // triggers; *over is set when the trigger buffer was too small.
 static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_total, bool *over, bool *need_full) {
@@ -1262,8 +1362,7 @@ static int finish_slot(tdf_engine *e, int slot, bool collect, int64_t *ntrig_tot
      const unsigned errf = (unsigned)(e->h_cnt[2 * slot + 1] & 0xffffffffu);
      if (errf & ERR_OVERFLOW)
           return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
-     if (errf & ERR_STAGE_TIMEOUT)
-          return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
+     TRY(wait_error(errf));
      if (errf & ERR_NEED_FULL_F) {
           *need_full = true;
           return TDF_OK;
@@ -1463,7 +1562,9 @@ static void autotune_cache_store(const tdf_engine *e) {
 // copy will deliver: the bounded wait of the pipeline kernels gives up after
 // `probes` probes and the kernel reports ERR_STAGE_TIMEOUT, as a pass whose
 // bulk copies never completed would.  No copy is issued, so nothing is in
-// flight when the kernel returns.
+// flight when the kernel returns.  Then lane 0 waits, as a fused pass's row
+// block does for its column blocks, on a count (err[1], zero) that nothing
+// raises, and reports ERR_ORDER_TIMEOUT when that wait gives up.
 __global__ void k_wait_probe(unsigned *err, int probes) {
      __shared__ __align__(8) uint64_t bar;
      if (threadIdx.x == 0) {
@@ -1474,6 +1575,7 @@ __global__ void k_wait_probe(unsigned *err, int probes) {
      if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);
      const bool done = mbar_wait(&bar, 0u, probes);
      if (!done && threadIdx.x == 0) atomicOr(err, ERR_STAGE_TIMEOUT);
+     if (threadIdx.x == 0 && !wait_count(err + 1, 1u, probes)) atomicOr(err, ERR_ORDER_TIMEOUT);
 }
 
 // ------------------------------------------------------------------ whole-call plans
@@ -1663,8 +1765,8 @@ int tdf_check_bounded_wait(int device, int32_t probes, uint32_t *status) {
      if (device < 0 || device >= ndev) return set_error(TDF_ERR_INVALID, "device %d of %d", device, ndev);
      CUCHK(cudaSetDevice(device));
      unsigned *d = nullptr;
-     CUCHK(cudaMalloc((void **)&d, sizeof(unsigned)));
-     cudaError_t ce = cudaMemset(d, 0, sizeof(unsigned));
+     CUCHK(cudaMalloc((void **)&d, 2 * sizeof(unsigned)));
+     cudaError_t ce = cudaMemset(d, 0, 2 * sizeof(unsigned));
      if (ce == cudaSuccess) {
           k_wait_probe<<<1, 32>>>(d, probes);
           ce = cudaGetLastError();
@@ -1762,6 +1864,10 @@ int tdf_engine_create(const tdf_segment *seg, const tdf_search_opts *opts, int f
      if (ff && ff[0] == '1') e->sparse_f = false;
      const char *rb = getenv("TDF_ROW_BULK");
      if (rb && rb[0] == '0') e->row_bulk = false;
+     const char *fp = getenv("TDF_FUSED_PASSES");
+     if (fp && fp[0] == '1') e->fused = true;
+     const char *fl = getenv("TDF_FUSE_LAG");
+     if (fl && atoi(fl) > 0) e->fuse_lag = atoi(fl);
      const char *gt = getenv("TDF_GROUP_TEMPLATES");
      if (gt && atoi(gt) > 0) e->Gt = std::min(atoi(gt), (int)tdf_engine::kGtMax);
      autotune_cache_lookup(e);
@@ -2097,8 +2203,7 @@ int tdf_search_segments_device(tdf_engine *e, int32_t nseg, const int32_t *slots
           const unsigned errf = (unsigned)((e->h_cnt[1] | e->h_cnt[3]) & 0xffffffffu);
           if (errf & ERR_OVERFLOW)
                return set_error(TDF_ERR_TRIGGER_OVERFLOW, "Too many triggers! buffer_size=%d [triggers]", e->opts.bufsize / 2);
-          if (errf & ERR_STAGE_TIMEOUT)
-               return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
+          TRY(wait_error(errf));
           if ((errf & ERR_NEED_FULL_F) && e->sparse_now) {
                e->sparse_now = false;   // once more with the full F store
                continue;
@@ -2231,8 +2336,7 @@ int tdf_fstat_spectrum(tdf_engine *e, int32_t pm, float mm, float nn, float ss, 
      TRY(run_templates(e, e->tparam.as<TmplParam>(), 1));
      CUCHK(cudaMemcpyAsync(e->h_cnt, e->counters[0].p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->stream));
      CUCHK(cudaStreamSynchronize(e->stream));
-     if (e->h_cnt[1] & ERR_STAGE_TIMEOUT)
-          return set_error(TDF_ERR_CUDA, "spindown stage: an asynchronous copy did not complete within its wait limit");
+     TRY(wait_error((unsigned)(e->h_cnt[1] & 0xffffffffu)));
      const int n = e->nF;
      if (e->form == TDF_FORM_SPLIT) {
           std::vector<float> f(n), mu(std::max(1, e->nblk_mu));

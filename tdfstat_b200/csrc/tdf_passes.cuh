@@ -63,19 +63,19 @@ struct has_tables : std::false_type {};
 template <class P>
 struct has_tables<P, std::void_t<decltype(P::kTables)>> : std::integral_constant<bool, P::kTables> {};
 
+// The column pass of CTA (blk, b): columns n2 = blk*LINES + c of batch b.
+// twline == nullptr: the line table is in shared memory already.
 template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
-__global__ void __launch_bounds__(pass_threads<L>(), (pass_min_blocks<T, L>()))
-k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
+__device__ __forceinline__ void col_body(const Pro &pro, const Epi &epi, const cx<T> *__restrict__ twline, int blk,
+                                         int b, unsigned char *smem_raw) {
      using G = LineGeom<T, L>;
-     extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
-     load_table<T>(tw, twline, L);
+     if (twline) load_table<T>(tw, twline, L);
      if constexpr (has_tables<Epi>::value) epi.template load_tables<L>(smem_raw);
      const int tid = threadIdx.x;
      const int c = tid % LINES, t = tid / LINES;
-     const int n2 = blockIdx.x * LINES + c;
-     const int b = blockIdx.y;
+     const int n2 = blk * LINES + c;
      cx<T> v[NA][8];
      if constexpr (is_staged<Pro>::value)
           pro.template load_staged<L>(v, b, n2, t, reinterpret_cast<unsigned char *>(lines),
@@ -93,32 +93,174 @@ k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ tw
           epi.template store<L>(v, b, n2, t);
 }
 
+// The row pass of CTA (blk, b): rows k1 = blk*LINES + c of batch b.
+// twline == nullptr: the line table is in shared memory already.  A bulk
+// source initialises its barrier itself (bar_init) or finds it initialised
+// and waits for the phase of `parity`.
 template <typename T, int L, int SIGN, int NA, class Src, class Epi>
-__global__ void __launch_bounds__(pass_threads<L>(), (row_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
+__device__ __forceinline__ void row_body(const Src &src, const Epi &epi, const cx<T> *__restrict__ twline, int blk,
+                                         int b, unsigned char *smem_raw, bool bar_init = true,
+                                         unsigned parity = 0u) {
      using G = LineGeom<T, L>;
-     extern __shared__ __align__(128) unsigned char smem_raw[];
      cx<T> *tw = reinterpret_cast<cx<T> *>(smem_raw);
      cx<T> *lines = tw + L;
      const int tid = threadIdx.x;
-     const int b = blockIdx.y;
-     const int k1b = blockIdx.x * LINES;
+     const int k1b = blk * LINES;
      const int c = tid % LINES, t = tid / LINES;
      cx<T> v[NA][8];
      cx<T> *s[NA];
      if constexpr (is_bulk<Src>::value) {
           src.template load_bulk<L>(v, b, k1b, c, t, reinterpret_cast<unsigned char *>(lines),
-                                    reinterpret_cast<uint64_t *>(smem_raw + src.bar_off), tw, twline);
+                                    reinterpret_cast<uint64_t *>(smem_raw + src.bar_off), tw, twline, bar_init,
+                                    parity);
      } else {
           // first-pass inputs straight from the rows into registers: per load
           // instruction a warp reads 4 consecutive elements of each of 8 rows
           src.template load<L>(v, b, k1b + c, t);
-          load_table<T>(tw, twline, L);
+          if (twline) load_table<T>(tw, twline, L);
      }
 #pragma unroll
      for (int a = 0; a < NA; a++) s[a] = lines + (a * LINES + c) * G::STRIDE;
      __syncthreads();
      line_fft<T, L, SIGN, NA>(v, s, tw, t);
      epi.template store<L>(v, b, k1b + c, t);
+}
+
+template <typename T, int L, int SIGN, int NA, class Pro, class Epi>
+__global__ void __launch_bounds__(pass_threads<L>(), (pass_min_blocks<T, L>()))
+k_colpass(const __grid_constant__ Pro pro, Epi epi, const cx<T> *__restrict__ twline) {
+     extern __shared__ __align__(128) unsigned char smem_raw[];
+     col_body<T, L, SIGN, NA>(pro, epi, twline, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+template <typename T, int L, int SIGN, int NA, class Src, class Epi>
+__global__ void __launch_bounds__(pass_threads<L>(), (row_min_blocks<T, L>())) k_rowpass(Src src, Epi epi, const cx<T> *__restrict__ twline) {
+     extern __shared__ __align__(128) unsigned char smem_raw[];
+     row_body<T, L, SIGN, NA>(src, epi, twline, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+// ------------------------------------------------------------------ fused pass order
+//
+// k_spinpass runs the column pass and the row pass of nt templates (FP32, two
+// arrays, N1 = N2 = L) as one launch of persistent CTAs (as many as are
+// resident at once).  C = R = L/LINES blocks per template and pass; the
+// items are handed out by tickets (ctl[0]) in the order
+//   col(0) .. col(D-1), then for b = 0 .. nt-D-1: col(b+D), row(b),
+//   then row(nt-D) .. row(nt-1)
+// (col(b) = the C column blocks of template b, row(b) its R row blocks), so
+// that a template's rows follow its columns by about D templates while its
+// spectra Y are still in L2.  A CTA takes its next ticket while it works on
+// the current item.  When a CTA starts the item after a column block of
+// template b, its thread 0 publishes that block (device-scope fence, then
+// ctl[2+b] += 1): the fence overlaps the new item instead of holding the
+// CTA.  A row block of template b waits until ctl[2+b] == C (bounded: on
+// time-out ERR_ORDER_TIMEOUT goes to *err and the block goes on).
+// No deadlock: a CTA publishes before it waits, and waits only for items of
+// smaller tickets; the waiting CTA whose current ticket is smallest depends
+// on items that are finished, current in CTAs that wait on nothing, or next
+// in CTAs whose current item has a smaller ticket and so is not waiting.
+// ctl is zeroed (memset) before each launch.
+constexpr unsigned ERR_ORDER_TIMEOUT = 8u;
+
+struct SpinOrder {
+     unsigned *ctl;   // [0] tickets, [1] unused, [2 + b] column blocks done of template b
+     unsigned *err;
+     int nt, C, R, D;
+     int limit;       // probes of a row block's wait
+};
+
+__device__ __forceinline__ void spin_item(const SpinOrder &o, unsigned k, int &b, int &blk, bool &row) {
+     const unsigned C = (unsigned)o.C, R = (unsigned)o.R, D = (unsigned)o.D;
+     const unsigned head = D * C;
+     if (k < head) {
+          row = false;
+          b = (int)(k / C);
+          blk = (int)(k % C);
+          return;
+     }
+     k -= head;
+     const unsigned mid = (unsigned)(o.nt - o.D) * (C + R);
+     if (k < mid) {
+          const unsigned g = k / (C + R), r = k % (C + R);
+          row = r >= C;
+          b = (int)(row ? g : g + D);
+          blk = (int)(row ? r - C : r);
+          return;
+     }
+     k -= mid;
+     row = true;
+     b = (int)((unsigned)(o.nt - o.D) + k / R);
+     blk = (int)(k % R);
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+     unsigned v;
+     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+     return v;
+}
+
+// orders this thread's generic-proxy accesses (and those it has observed)
+// before the bulk copies it issues next, in global and shared memory
+__device__ __forceinline__ void fence_proxy_async() {
+     asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+// Waits until *p >= target, giving up after `limit` probes; returns false
+// when it gave up.
+__device__ __forceinline__ bool wait_count(const unsigned *p, unsigned target, int limit) {
+     for (int it = 0; it < limit; it++) {
+          if (ld_acquire_gpu(p) >= target) return true;
+          __nanosleep(64);
+     }
+     return ld_acquire_gpu(p) >= target;
+}
+
+template <int L, class Pro, class EpiC, class Src, class EpiR>
+__global__ void __launch_bounds__(pass_threads<L>(), (L <= 256 ? 4 : 2))
+k_spinpass(const __grid_constant__ Pro pro, const __grid_constant__ EpiC epic, const __grid_constant__ Src src,
+           const __grid_constant__ EpiR epir, const float2 *__restrict__ twline, const __grid_constant__ SpinOrder o) {
+     extern __shared__ __align__(128) unsigned char smem_raw[];
+     __shared__ unsigned s_tk[2];
+     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + src.bar_off);
+     const unsigned total = (unsigned)o.nt * (unsigned)(o.C + o.R);
+     if (threadIdx.x == 0) {
+          s_tk[0] = atomicAdd(&o.ctl[0], 1u);
+          mbar_init(bar, 1);
+          mbar_fence_init();
+     }
+     // one line table serves both passes (N1 = N2)
+     load_table<float>(reinterpret_cast<float2 *>(smem_raw), twline, L);
+     __syncthreads();
+     int pend = -1;         // template of the column block finished last, not yet published
+     unsigned nrow = 0;     // row items done (barrier phase)
+     for (int it = 0;; it++) {
+          const unsigned k = s_tk[it & 1];
+          if (threadIdx.x == 0) {
+               if (pend >= 0) {
+                    __threadfence();
+                    atomicAdd(&o.ctl[2 + pend], 1u);
+               }
+               if (k < total) s_tk[(it + 1) & 1] = atomicAdd(&o.ctl[0], 1u);
+          }
+          pend = -1;
+          if (k >= total) break;
+          int b, blk;
+          bool row;
+          spin_item(o, k, b, blk, row);
+          if (!row) {
+               col_body<float, L, -1, 2>(pro, epic, (const float2 *)nullptr, blk, b, smem_raw);
+               pend = b;
+          } else {
+               if (threadIdx.x == 0) {
+                    if (!wait_count(&o.ctl[2 + b], (unsigned)o.C, o.limit)) atomicOr(o.err, ERR_ORDER_TIMEOUT);
+                    fence_proxy_async();
+               }
+               __syncthreads();
+               row_body<float, L, -1, 2>(src, epir, (const float2 *)nullptr, blk, b, smem_raw, false, nrow & 1u);
+               nrow++;
+          }
+          __syncthreads();   // the item's shared memory is free; the next ticket is visible
+     }
 }
 
 // ------------------------------------------------------------------ policies
@@ -260,15 +402,18 @@ struct RowsYBulk {
 
      template <int L>
      __device__ __forceinline__ void load_bulk(cx<T> (&v)[2][8], int b, int k1b, int c, int t, unsigned char *stage,
-                                               uint64_t *bar, cx<T> *tw, const cx<T> *twline) const {
+                                               uint64_t *bar, cx<T> *tw, const cx<T> *twline, bool init = true,
+                                               unsigned parity = 0u) const {
           constexpr unsigned RB = EB * L;   // bytes of a row
           static_assert(stage_bytes<L>() <= sizeof(cx<T>) * 2 * LINES * LineGeom<T, L>::STRIDE,
                         "row slots must fit in the line buffers");
-          if (threadIdx.x == 0) {
-               mbar_init(bar, 1);
-               mbar_fence_init();
+          if (init) {
+               if (threadIdx.x == 0) {
+                    mbar_init(bar, 1);
+                    mbar_fence_init();
+               }
+               __syncthreads();   // the barrier is initialised before anyone waits on it
           }
-          __syncthreads();   // the barrier is initialised before anyone waits on it
           if (threadIdx.x == 0) {
                mbar_expect_tx(bar, LINES * RB);
                const cx<T> *r0 = y + ((size_t)b * N + (size_t)k1b * rowstride) * 2;
@@ -276,8 +421,8 @@ struct RowsYBulk {
                for (int r = 0; r < LINES; r++)
                     bulk_load(stage + r * (RB + kPad), r0 + (size_t)r * rowstride * 2, RB, bar);
           }
-          load_table<T>(tw, twline, L);
-          const bool ok = mbar_wait(bar, 0u);
+          if (twline) load_table<T>(tw, twline, L);
+          const bool ok = mbar_wait(bar, parity);
           const unsigned char *row = stage + c * (RB + kPad);
 #pragma unroll
           for (int m = 0; m < 8; m++) {

@@ -67,8 +67,9 @@ class Workload:
     all inside the grid), so that each rank's contiguous shard is one full
     patch: the work per GPU is fixed as the GPU count grows."""
 
-    def __init__(self, name: str, root: str, world: int = 1):
-        case, (nm, nn_), nspd, step = workload_case(name)
+    def __init__(self, name: str, root: str, world: int = 1, case=None):
+        # case: (synth.Case, patch shape, spindowns, step) instead of the named workload's
+        case, (nm, nn_), nspd, step = case if case is not None else workload_case(name)
         self.name, self.case = name, case
         inj = case.injections[0] if case.injections else None
         c = case

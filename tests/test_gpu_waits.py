@@ -1,7 +1,9 @@
-"""Failure detection of the asynchronous-copy waits, without a GPU fault: a
-warp waits on a barrier whose copy never arrives (nothing is issued); the
-bounded wait gives up after a short limit, the kernel reports
-TDF_WAIT_TIMEOUT_BIT, the host reads it, and the device stays usable."""
+"""Failure detection of the bounded waits, without a GPU fault: a warp waits
+on a barrier whose copy never arrives (nothing is issued), then one thread on
+a block count that nothing raises (the fused passes' row-block wait); each
+wait gives up after a short limit, the kernel reports TDF_WAIT_TIMEOUT_BIT
+and TDF_ORDER_TIMEOUT_BIT, the host reads them, and the device stays
+usable."""
 import ctypes as C
 import time
 
@@ -12,6 +14,7 @@ from tdfstat_b200 import _abi
 pytestmark = pytest.mark.gpu
 
 TDF_WAIT_TIMEOUT_BIT = 2
+TDF_ORDER_TIMEOUT_BIT = 8
 
 
 def test_wait_gives_up_and_reports(golden):
@@ -22,6 +25,7 @@ def test_wait_gives_up_and_reports(golden):
     assert lib.tdf_check_bounded_wait(0, 1000, C.byref(st)) == _abi.TDF_OK
     assert time.monotonic() - t0 < 5.0
     assert st.value & TDF_WAIT_TIMEOUT_BIT
+    assert st.value & TDF_ORDER_TIMEOUT_BIT
     # the context is intact: a search right after gives its records
     g = golden("g2_h1l1_inj")
     eng = Engine.from_job(g.job32, form="split")

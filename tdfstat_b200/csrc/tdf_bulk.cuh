@@ -81,4 +81,18 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
          : "memory");
 }
 
+// Per-thread asynchronous copies global -> shared memory of 16 or 8 bytes
+// (both addresses aligned to the size), waited for with cp_async_wait_all();
+// a thread's copies are all in flight at once and hold no registers.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"((uint64_t)src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"((uint64_t)src) : "memory");
+}
+// the calling thread's copies have landed (other threads' need a barrier)
+__device__ __forceinline__ void cp_async_wait_all() {
+     asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 }  // namespace tdf

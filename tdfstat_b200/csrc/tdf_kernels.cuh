@@ -262,8 +262,12 @@ __global__ void __launch_bounds__(256) k_sky_sums(const double *__restrict__ par
 // so the start-up error is below 1e-27 of the values after 48 steps and the
 // results are those of one sequential sweep.  A CTA of SPL_T threads stages
 // its tile of the inputs (and the warm-up margin) in shared memory with
-// coalesced loads; lane j then reads index j*SPL_K + r, and one pad word per
-// 16 elements puts the lanes of a wavefront on distinct banks.
+// per-thread asynchronous copies (all in flight at once); lane j then reads
+// index j*SPL_K + r, and one pad word per 16 elements puts the lanes of a
+// wavefront on distinct banks.  A thread keeps its SPL_K outputs in
+// registers until the whole CTA is done reading the staged inputs, writes
+// them over the tile's part of the staging buffer, and the CTA stores the
+// tile with consecutive lanes on consecutive indices.
 constexpr int SPL_T = 64;                  // threads per CTA
 constexpr int SPL_K = 16;                  // indices per thread
 constexpr int SPL_W = 48;                  // warm-up steps
@@ -277,8 +281,8 @@ __global__ void __launch_bounds__(SPL_T) k_spline_fwd(const double2 *__restrict_
 {
      constexpr int S = SPL_TILE + SPL_W + 2;   // staged samples: [tile0 - W - 1, tile0 + TILE + 1)
      constexpr int P = SPL_TILE + SPL_W;       // staged factors:  [tile0 - W, tile0 + TILE)
-     __shared__ double2 ys[S + S / 16 + 1];
-     __shared__ double ps[P + P / 16 + 1];
+     __shared__ __align__(16) double2 ys[S + S / 16 + 1];
+     __shared__ __align__(16) double ps[P + P / 16 + 1];
      const int arr = blockIdx.y;
      const double2 *y = Z + (size_t)arr * stride;
      double2 *u = U + (size_t)arr * stride;
@@ -286,30 +290,52 @@ __global__ void __launch_bounds__(SPL_T) k_spline_fwd(const double2 *__restrict_
      const int yb = tile0 - SPL_W - 1, pb = tile0 - SPL_W;
      for (int k = threadIdx.x; k < S; k += SPL_T) {
           const int i = yb + k;
-          if (i >= 0 && i < n) ys[spl_pad(k)] = y[i];
+          if (i >= 0 && i < n) cp_async16(&ys[spl_pad(k)], &y[i]);
      }
      for (int k = threadIdx.x; k < P; k += SPL_T) {
           const int i = pb + k;
-          if (i >= 0 && i < n) ps[spl_pad(k)] = pco[i];
+          if (i >= 0 && i < n) cp_async8(&ps[spl_pad(k)], &pco[i]);
      }
+     cp_async_wait_all();
      __syncthreads();
      const int lo = tile0 + threadIdx.x * SPL_K;
-     if (lo >= n) return;
      const int hi = min(n - 1, lo + SPL_K);
-     if (lo == 0) u[0] = make_double2(0., 0.);
-     const int i0 = max(1, lo - SPL_W);
-     double ur = 0., ui = 0.;
-     double2 ym = ys[spl_pad(i0 - 1 - yb)], y0 = ys[spl_pad(i0 - yb)];
-     for (int i = i0; i < hi; i++) {
-          const double2 yp = ys[spl_pad(i + 1 - yb)];
-          const double p = ps[spl_pad(i - pb)];
-          const double dr = ym.x - 2. * y0.x + yp.x;
-          const double dI = ym.y - 2. * y0.y + yp.y;
-          ur = (-.5 * ur + 3. * dr) * p;
-          ui = (-.5 * ui + 3. * dI) * p;
-          if (i >= lo) u[i] = make_double2(ur, ui);
-          ym = y0;
-          y0 = yp;
+     double2 out[SPL_K];
+     if (lo < n) {
+          const int i0 = max(1, lo - SPL_W);
+          double ur = 0., ui = 0.;
+          double2 ym = ys[spl_pad(i0 - 1 - yb)], y0 = ys[spl_pad(i0 - yb)];
+          auto step = [&](int i) {
+               const double2 yp = ys[spl_pad(i + 1 - yb)];
+               const double p = ps[spl_pad(i - pb)];
+               const double dr = ym.x - 2. * y0.x + yp.x;
+               const double dI = ym.y - 2. * y0.y + yp.y;
+               ur = (-.5 * ur + 3. * dr) * p;
+               ui = (-.5 * ui + 3. * dI) * p;
+               ym = y0;
+               y0 = yp;
+          };
+          for (int i = i0; i < lo; i++) step(i);   // warm-up
+#pragma unroll
+          for (int r = 0; r < SPL_K; r++) {
+               const int i = lo + r;
+               out[r] = make_double2(0., 0.);      // u[0] = 0
+               if (i >= i0 && i < hi) {
+                    step(i);
+                    out[r] = make_double2(ur, ui);
+               }
+          }
+     }
+     __syncthreads();   // every thread is done with the staged samples
+     if (lo < n) {
+#pragma unroll
+          for (int r = 0; r < SPL_K; r++)
+               if (lo + r < hi || lo + r == 0) ys[spl_pad(lo + r - yb)] = out[r];
+     }
+     __syncthreads();
+     for (int k = threadIdx.x; k < SPL_TILE; k += SPL_T) {
+          const int i = tile0 + k;
+          if (i < n - 1) u[i] = ys[spl_pad(k + SPL_W + 1)];
      }
 }
 
@@ -320,8 +346,8 @@ __global__ void __launch_bounds__(SPL_T) k_spline_bwd(const double2 *__restrict_
                                                       size_t stride, const double *__restrict__ gco, int n)
 {
      constexpr int S = SPL_TILE + SPL_W;       // staged: [tile0, tile0 + TILE + W)
-     __shared__ double2 us[S + S / 16 + 1];
-     __shared__ double gs[S + S / 16 + 1];
+     __shared__ __align__(16) double2 us[S + S / 16 + 1];
+     __shared__ __align__(16) double gs[S + S / 16 + 1];
      const int arr = blockIdx.y;
      const double2 *u = U + (size_t)arr * stride;
      double2 *y2 = Y2 + (size_t)arr * stride;
@@ -329,23 +355,45 @@ __global__ void __launch_bounds__(SPL_T) k_spline_bwd(const double2 *__restrict_
      for (int k = threadIdx.x; k < S; k += SPL_T) {
           const int i = tile0 + k;
           if (i < n) {
-               us[spl_pad(k)] = u[i];
-               gs[spl_pad(k)] = gco[i];
+               cp_async16(&us[spl_pad(k)], &u[i]);
+               cp_async8(&gs[spl_pad(k)], &gco[i]);
           }
      }
+     cp_async_wait_all();
      __syncthreads();
      const int lo = tile0 + threadIdx.x * SPL_K;
-     if (lo >= n) return;
      const int hi = min(n, lo + SPL_K);
-     const int ks = min(n - 1, hi + SPL_W);
-     if (ks == n - 1 && ks < hi) y2[n - 1] = make_double2(0., 0.);
-     double yr = 0., yi = 0.;
-     for (int k = ks - 1; k >= lo; k--) {
-          const double g = gs[spl_pad(k - tile0)];
-          const double2 uk = us[spl_pad(k - tile0)];
-          yr = g * yr + uk.x;
-          yi = g * yi + uk.y;
-          if (k < hi) y2[k] = make_double2(yr, yi);
+     double2 out[SPL_K];
+     if (lo < n) {
+          const int ks = min(n - 1, hi + SPL_W);
+          double yr = 0., yi = 0.;
+          auto step = [&](int k) {
+               const double g = gs[spl_pad(k - tile0)];
+               const double2 uk = us[spl_pad(k - tile0)];
+               yr = g * yr + uk.x;
+               yi = g * yi + uk.y;
+          };
+          for (int k = ks - 1; k >= hi; k--) step(k);   // warm-up
+#pragma unroll
+          for (int r = SPL_K - 1; r >= 0; r--) {
+               const int k = lo + r;
+               out[r] = make_double2(0., 0.);      // y2[n-1] = 0
+               if (k < hi && k < ks) {
+                    step(k);
+                    out[r] = make_double2(yr, yi);
+               }
+          }
+     }
+     __syncthreads();   // every thread is done with the staged inputs
+     if (lo < n) {
+#pragma unroll
+          for (int r = 0; r < SPL_K; r++)
+               if (lo + r < hi) us[spl_pad(lo + r - tile0)] = out[r];
+     }
+     __syncthreads();
+     for (int k = threadIdx.x; k < SPL_TILE; k += SPL_T) {
+          const int i = tile0 + k;
+          if (i < n) y2[i] = us[spl_pad(k)];
      }
 }
 

@@ -6,8 +6,9 @@ a template's row blocks follow its column blocks by `lag` templates and wait
 (bounded) until all of them have stored their spectra.  The arithmetic is the
 two passes' own, in the same order, so the records must equal those of the
 two launches (TDF_FUSED_PASSES=0) bit for bit: for chunk sizes that do and do
-not divide the template count, lags from 1 to past the chunk, and both F
-stores (sparse default, full with TDF_FULL_F=1)."""
+not divide the template count, lags from 1 to past the chunk, both F
+stores (sparse default, full with TDF_FULL_F=1), and an F range past
+nfftf/2 (whole rows kept)."""
 import shutil
 import tempfile
 
@@ -72,4 +73,18 @@ def test_fused_passes_match_two_launches(wl, monkeypatch, tc, lag):
 def test_fused_passes_full_f_store(wl, monkeypatch):
     two, _ = _search(wl, monkeypatch, False, 32, full_f=True)
     one, _ = _search(wl, monkeypatch, True, 32, full_f=True)
+    _same(one, two)
+
+
+def test_fused_passes_whole_rows(wl, monkeypatch):
+    """An F range reaching past nfftf/2: the row blocks keep every output of
+    their rows (no half-row pruning)."""
+    fr = list(wl.job.range.fr)
+    try:
+        wl.job.range.fr = [fr[0], wl.job.sett.nfftf // 2 + 4096]
+        two, _ = _search(wl, monkeypatch, False, 32)
+        one, _ = _search(wl, monkeypatch, True, 32)
+    finally:
+        wl.job.range.fr = fr
+    assert sum(len(p) for p in two[1]) > 0
     _same(one, two)

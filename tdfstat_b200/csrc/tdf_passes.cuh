@@ -8,6 +8,9 @@
 //   k_rowpass<T, L, SIGN, NA, Src, Epi>: CTA = LINES rows k1 of an
 //     N = N1*L transform, L threads; the first-pass inputs are loaded from
 //     the rows straight into registers, Epi::store consumes X[k1 + N1*k2].
+//   k_spinpass<L, ...>: both passes of the FP32 spindown transform (N1 = N2
+//     = L) as one launch of persistent CTAs taking column and row blocks in
+//     ticket order (opt-in; see the comment above its definition).
 #pragma once
 
 #include <type_traits>

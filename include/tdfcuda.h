@@ -120,6 +120,14 @@ typedef struct tdf_engine tdf_engine;
    set when the waits gave up, as they must).  The device stays usable. */
 int tdf_check_bounded_wait(int device, int32_t probes, uint32_t *status);
 
+/* Diagnostic (no device needed): the item that ticket `ticket` names in a
+   fused pass launch (TDF_FUSED_PASSES=1) of `nt` templates with `blocks`
+   column and `blocks` row blocks per template and a row lag of `lag`
+   templates (clamped to [1, nt] as the launcher does): template *tmpl,
+   block *block, *row = 1 for a row block.  The same code the kernel runs. */
+int tdf_spin_order_item(int32_t nt, int32_t blocks, int32_t lag, uint32_t ticket, int32_t *tmpl, int32_t *block,
+                        int32_t *row);
+
 const char *tdf_status_string(int status);
 /* message of the calling thread's last failed call ("" if none) */
 const char *tdf_last_error(void);

@@ -169,6 +169,8 @@ RECP = C.POINTER(TdfRecord)
 
 ABI_FUNCTIONS = [
     ("tdf_check_bounded_wait", C.c_int, [C.c_int, C.c_int32, C.POINTER(C.c_uint32)]),
+    ("tdf_spin_order_item", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     ("tdf_status_string", C.c_char_p, [C.c_int]),
     ("tdf_last_error", C.c_char_p, []),
     ("tdf_device_count", C.c_int, [I32P]),

@@ -1754,6 +1754,22 @@ static int plan_check(tdf_engine *e, const std::vector<PlanPoint> &hp, const std
 
 extern "C" {
 
+int tdf_spin_order_item(int32_t nt, int32_t blocks, int32_t lag, uint32_t ticket, int32_t *tmpl, int32_t *block,
+                        int32_t *row) {
+     if (!tmpl || !block || !row || nt < 1 || blocks < 1 || lag < 1 ||
+         (int64_t)nt * blocks * 2 > (int64_t)UINT32_MAX || (int64_t)ticket >= (int64_t)nt * blocks * 2)
+          return set_error(TDF_ERR_INVALID, "outputs must be non-null, nt, blocks, lag >= 1 and ticket < 2*nt*blocks");
+     // the launcher's order: C = R = blocks per template, lag clamped to [1, nt]
+     SpinOrder o{nullptr, nullptr, nt, blocks, blocks, std::max(1, std::min(lag, nt)), 0};
+     int b = 0, blk = 0;
+     bool r = false;
+     spin_item(o, ticket, b, blk, r);
+     *tmpl = b;
+     *block = blk;
+     *row = r ? 1 : 0;
+     return TDF_OK;
+}
+
 int tdf_check_bounded_wait(int device, int32_t probes, uint32_t *status) {
      if (!status || probes < 1 || probes > (1 << 20))
           return set_error(TDF_ERR_INVALID, "status must be non-null and probes in 1..2^20");

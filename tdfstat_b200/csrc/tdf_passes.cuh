@@ -172,7 +172,7 @@ struct SpinOrder {
      int limit;       // probes of a row block's wait
 };
 
-__device__ __forceinline__ void spin_item(const SpinOrder &o, unsigned k, int &b, int &blk, bool &row) {
+__host__ __device__ __forceinline__ void spin_item(const SpinOrder &o, unsigned k, int &b, int &blk, bool &row) {
      const unsigned C = (unsigned)o.C, R = (unsigned)o.R, D = (unsigned)o.D;
      const unsigned head = D * C;
      if (k < head) {
